@@ -1,0 +1,334 @@
+"""Benchmark: refactorization + FP64-refined solve on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mesh|nodal|batch]
+
+One step = refactorize with a new value set of the same pattern (values placed
+into the LU layout on the GPU, FP32 factorization) + FP64-refined solve of the
+step's right-hand sides to the workload's residual tolerance.  ``value`` is
+solves per second over all GPUs with inputs resident in HBM; ``e2e`` is the
+same through the public API with host buffers (copies inside the timed
+region).  ``--impl reference`` times NICSLU, the reference's own CPU solver,
+on the same workload on this host's cores (rank 0 only).
+
+Workloads (seeded synthetic matrices):
+  mesh   700 x 700 resistive power grid, n = 490,000, 1 right-hand side,
+         refinement to 1e-12 (default);
+  nodal  nodal-analysis matrix n = 4,960, 1 right-hand side, 1e-10;
+  batch  256 value sets of one n = 20,000 nodal pattern, 4 right-hand sides
+         each, 1e-10.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "glu-hcu_b200"))
+
+METRIC = "refactor ms & batched solves/s at 1e-10 FP64 residual vs plain FP32 on B200"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="mesh", choices=["mesh", "nodal", "batch"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(name):
+    from pyglu import synth
+
+    if name == "mesh":
+        A = synth.config1()
+        return dict(A=A, batch=1, nrhs=1, tol=1e-12, values=2,
+                    desc="power-grid mesh 700x700, n=490000, 1 RHS, refine to 1e-12",
+                    b=lambda n, k, s: synth.rhs_loads(n, seed=s)[None, :])
+    if name == "nodal":
+        A = synth.config0()
+        return dict(A=A, batch=1, nrhs=1, tol=1e-10, values=2,
+                    desc="nodal matrix n=4960, 1 RHS, refine to 1e-10",
+                    b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
+    A = synth.config2_pattern()
+    return dict(A=A, batch=256, nrhs=4, tol=1e-10, values=1,
+                desc="256 value sets of one nodal pattern n=20000, 4 RHS each, refine to 1e-10",
+                b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x, pg, device):
+    if pg is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_reference(W, steps, warmup, sample_only=False):
+    """NICSLU (reference CPU code) refactor + solve + refine on this host."""
+    import oracle
+    from pyglu import synth
+
+    data, indices, indptr, n = W["A"]
+    threads = os.cpu_count() or 1
+    vals = synth.perturb_values(data, indices, indptr, n, count=2, seed=7)
+    b = W["b"](n, W["nrhs"], 11)
+    nl = oracle.RefNicsLU(data, indices, indptr, n, threads)
+    per_step_solves = W["nrhs"] if sample_only or W["batch"] == 1 else W["nrhs"]
+
+    def step(i):
+        nl.refactor(vals[i % 2])
+        for k in range(W["nrhs"]):
+            x = nl.solve(b[k])
+            nl.refine(x, b[k], W["tol"], 10)
+
+    for i in range(warmup):
+        step(i)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        step(i)
+    dt = (time.perf_counter() - t0) / steps
+    sample = (f"{steps} step(s) of NICSLU ReFactorize_MT + Solve + Refine on one value set "
+              f"({per_step_solves} RHS) of the workload matrix")
+    return per_step_solves / dt, dt, threads, sample
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    W = workload(args.workload)
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, dt, thr, sample = cpu_reference(W, args.steps, args.warmup)
+        line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": W["desc"], "solver": "NICSLU (reference CPU code)"},
+                "cpu_baseline": {"value": v, "unit": "solves/s", "cores": thr, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    import pyglu
+    from pyglu import _capi, synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    data, indices, indptr, n = W["A"]
+    B, nrhs = W["batch"], W["nrhs"]
+    nvals = max(W["values"], 1)
+    vals = synth.perturb_values(data, indices, indptr, n, count=max(B, 2), seed=7)
+    if B == 1:
+        lu = pyglu.GLUFactorization(vals[0], indices, indptr, n, device=local)
+        handle = lu.handle
+    else:
+        lu = pyglu.BatchedGLU(indices, indptr, n, vals[:B], device=local)
+        handle = lu.handle
+    an = lu._an
+    eng = _capi.engine()
+    stream = torch.cuda.current_stream(dev)
+    sp_ = _capi.C.c_void_p(stream.cuda_stream)
+    # device-resident inputs: value sets and right-hand sides
+    if B == 1:
+        d_vals = [torch.tensor(vals[i], dtype=torch.float64, device=dev) for i in range(nvals)]
+    else:
+        d_vals = [torch.tensor(vals[:B], dtype=torch.float64, device=dev)]
+    b_host = np.ascontiguousarray(np.broadcast_to(W["b"](n, nrhs, 11), (B, nrhs, n)))
+    d_b = torch.tensor(b_host, dtype=torch.float64, device=dev)
+    d_x = torch.empty_like(d_b)
+    rst = _capi.RefineStats()
+    st = _capi.Stats()
+
+    def step(i):
+        v = d_vals[i % len(d_vals)]
+        _capi.check(eng.glu_load_source_values(handle, 0, B, _capi.C.c_void_p(v.data_ptr()), _capi.GLU_DEVICE, sp_))
+        _capi.check(eng.glu_factor(handle, 0, B, 0, sp_), "factor")
+        s = eng.glu_solve_refined(handle, 0, B, nrhs, _capi.C.c_void_p(d_b.data_ptr()),
+                                  _capi.C.c_void_p(d_x.data_ptr()), W["tol"], 10, 0, _capi.GLU_DEVICE,
+                                  _capi.C.byref(rst), sp_)
+        if s not in (0, _capi.GLU_ERR_NOT_CONVERGED):
+            _capi.check(s, "refined solve")
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fact_ms = []
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(i)
+        eng.glu_get_stats(handle, _capi.C.byref(st))
+        fact_ms.append(st.last_factor_ms)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if pg:
+        pg.barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, pg, dev)
+    solves = B * nrhs
+    value = world * solves / (ms / 1e3)
+    residual = rst.residual
+    iters = rst.iterations
+
+    # plain FP32 form: factor + unrefined solve per matrix (for the comparison)
+    eng.glu_get_stats(handle, _capi.C.byref(st))
+    factor_ms = float(np.median(fact_ms))
+    # solve-only time (refined), device events
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s = eng.glu_solve_refined(handle, 0, B, nrhs, _capi.C.c_void_p(d_b.data_ptr()), _capi.C.c_void_p(d_x.data_ptr()),
+                              W["tol"], 10, 0, _capi.GLU_DEVICE, _capi.C.byref(rst), sp_)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    solve_ms = e0.elapsed_time(e1)
+
+    # e2e through the public API with host buffers
+    e2e_steps = max(1, min(args.steps, 3))
+    if B == 1:
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for i in range(e2e_steps):
+            lu.refactor(vals[i % nvals])
+            x = lu.solve(b_host[0].T if nrhs > 1 else b_host[0, 0], refine=True, tol=W["tol"])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / e2e_steps
+        h2d = vals[0].nbytes + b_host[0].nbytes
+        d2h = b_host[0].nbytes
+    else:
+        t0 = time.perf_counter()
+        for i in range(e2e_steps):
+            lu.refactor(vals[:B])
+            X = lu.solve(b_host, tol=W["tol"])
+        torch.cuda.synchronize()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+        h2d = vals[:B].nbytes + b_host.nbytes
+        d2h = b_host.nbytes
+    e2e_ms = max_over_ranks(e2e_ms, pg, dev)
+    e2e_value = world * solves / (e2e_ms / 1e3)
+
+    # roofline of the factorization (all its kernels, one launch sequence)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    nnz_lu = an.nnz_lu
+    alg_bytes = (8.0 * B + 8.0) * nnz_lu  # values read+written per set, row + CSR index once
+    achieved = alg_bytes / (factor_ms / 1e3) / 1e9
+    flops = st.factor_flops * B
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": None, "kernel": "factorization (all kernels of one glu_factor call)",
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "fp32_tflops": flops / (factor_ms / 1e3) / 1e12}
+
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": W["desc"], "n": n, "nnz_lu": nnz_lu, "batch": B, "nrhs": nrhs,
+                       "levels": st.num_lev, "dense_tail": st.dense_tail, "l2": "inputs larger than L2",
+                       "parallelism": f"replicas x{world}" if B == 1 else f"batch x{world}"},
+            "refactor_ms": factor_ms, "solve_refined_ms": solve_ms, "residual": residual,
+            "refine_iterations": iters, "refine_dtype": "f64",
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": roof, "gpu_launches": int(st.factor_launches) * args.steps, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+
+            if oracle.ref_available():
+                v, dt, thr, sample = cpu_reference(W, 1, 0, sample_only=True)
+                line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": thr, "kind": "reference",
+                                        "sample": sample}
+        except Exception as e:  # pragma: no cover
+            line["cpu_baseline"] = {"error": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

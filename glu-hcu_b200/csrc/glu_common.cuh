@@ -1,0 +1,83 @@
+// Device-side structures and helpers shared by the GLU kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace glu {
+
+// Device copy of the L+U pattern (Symbolic_Matrix arrays plus csr_pos).
+struct DevPattern {
+    const uint32_t *cptr;   // sym_c_ptr[n+1]
+    const uint32_t *ridx;   // sym_r_idx[nnz]
+    const uint32_t *diag;   // l_col_ptr[n]
+    const uint32_t *rptr;   // csr_r_ptr[n+1]
+    const uint32_t *cidx;   // csr_c_idx[nnz]
+    const uint32_t *rdiag;  // csr_diag_ptr[n]
+    const uint32_t *cpos;   // CSC position of every CSR entry
+    uint32_t n;
+    uint32_t nnz;
+};
+
+// Device status word bits (set with atomicOr, read back by the host).
+enum : uint32_t {
+    DEV_ZERO_PIVOT = 1u,
+    DEV_NONFINITE_PIVOT = 2u,
+    DEV_TIMEOUT = 4u,
+    DEV_BAD_INDEX = 8u,
+};
+
+// Upper bound on spins of any device-side wait before it gives up and
+// reports DEV_TIMEOUT (each spin sleeps ~64-256 ns: a few seconds in total).
+constexpr uint32_t kSpinLimit = 1u << 24;
+
+#ifdef __CUDACC__
+__device__ __forceinline__ float ld_cg(const float *p) { return __ldcg(p); }
+__device__ __forceinline__ void st_cg(float *p, float v) { __stcg(p, v); }
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int32_t ld_acquire_gpu(const int32_t *p) {
+    int32_t v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_gpu(int32_t *p, int32_t v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// First index in [lo, hi] (inclusive, hi is a valid answer) with a[idx] >= key.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t lo,
+                                                    uint32_t hi, uint32_t key) {
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Last s in [lo, hi) with off[s] <= key (off ascending, off[lo] <= key).
+__device__ __forceinline__ uint32_t upper_slot(const uint32_t *__restrict__ off, uint32_t lo,
+                                               uint32_t hi, uint32_t key) {
+    // invariant: off[lo] <= key, answer in [lo, hi)
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= key)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+#endif  // __CUDACC__
+
+}  // namespace glu

@@ -1,0 +1,928 @@
+// Host side of libglu_b200: handles, schedule planning and the C ABI.
+//
+// One handle replaces the per-call work of LUonDevice (src/numeric.cu:347-639):
+// the pattern is uploaded once, the level sets are built on the GPU, and the
+// factorization schedule is planned once; every factorization then only
+// enqueues kernels on the caller's stream (no allocation, no per-level host
+// synchronization, numeric.cu:615-616).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "glu_internal.h"
+#include "glu_kernels.h"
+
+namespace glu {
+
+static thread_local std::string g_last_error;
+
+Status set_error(Status s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+static Status cuda_fail(cudaError_t e, const char *what) {
+    return set_error(e == cudaErrorMemoryAllocation ? GLU_ERR_NOMEM : GLU_ERR_CUDA, "%s: %s", what,
+                     cudaGetErrorString(e));
+}
+
+#define GLU_CUDA(call, what)                                  \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, (what));  \
+    } while (0)
+
+// Device buffer owned by a handle.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t b) {
+        release();
+        if (b == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    cudaError_t ensure(size_t b) { return b <= bytes ? cudaSuccess : alloc(b); }
+    template <class T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
+template <class T>
+static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
+    cudaError_t e = d.alloc(sizeof(T) * std::max<size_t>(h.size(), 1));
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpy(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
+}
+
+enum StepKind { STEP_LEVEL = 0, STEP_CHAIN = 1 };
+struct Step {
+    int kind;
+    uint32_t l0, l1;  // sparse levels [l0, l1)
+};
+
+}  // namespace glu
+
+using namespace glu;
+
+struct glu_symbolic_s {
+    SymbolicData s;
+};
+
+struct glu_handle_s {
+    int device = 0;
+    uint32_t n = 0, nnz = 0, batch = 1;
+    SymbolicData pat;  // host copy of the pattern (csr_pos included)
+    DevBuf d_cptr, d_ridx, d_diag, d_rptr, d_cidx, d_rdiag, d_cpos;
+    DevPattern P{};
+    DevBuf d_val;
+    // levels
+    int32_t num_lev = 0;
+    std::vector<int32_t> level_ptr, level_idx;
+    // factor plan
+    glu_tuning tune{};
+    uint32_t t = 0, m = 0;
+    std::vector<uint32_t> doff_h;
+    DevBuf d_doff, d_sched, d_item_off, d_levels;
+    std::vector<LevelInfo> levels_h;
+    std::vector<uint32_t> items_h;
+    std::vector<uint64_t> work_h;
+    std::vector<Step> steps;
+    uint32_t chain_cluster = 8;
+    FactorPlanDev F{};
+    double flops = 0;
+    // solve plan
+    DevBuf d_lneed, d_uneed;
+    SolvePlanDev S{};
+    // transforms (forward in/out, transposed in/out)
+    DevBuf d_tr[8];
+    TransformDev T{};
+    bool has_transform = false;
+    // source matrix A0
+    bool has_source = false;
+    uint32_t nnz_src = 0;
+    DevBuf d_src_lu, d_src_scale, d_a0_rptr, d_a0_cidx, d_a0_vmap, d_a0_cptr, d_a0_ridx, d_a0_ident, d_ax0;
+    bool ax0_loaded = false;
+    // work buffers
+    DevBuf d_status, d_pert, d_colmax, d_diag_scratch, d_counters, d_ticket, d_y, d_io32, d_b64,
+        d_x64, d_r64, d_norms;
+    uint32_t *h_status = nullptr;  // pinned
+    double *h_norms = nullptr;     // pinned
+    size_t h_norms_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool factored = false;
+    glu_stats stats{};
+
+    ~glu_handle_s() {
+        if (h_status) cudaFreeHost(h_status);
+        if (h_norms) cudaFreeHost(h_norms);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline cudaStream_t S_(glu_stream s) { return static_cast<cudaStream_t>(s); }
+
+// Largest trailing block [t, n) in which every entry is in the pattern.
+void find_dense_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t &m) {
+    const uint32_t n = s.n;
+    // run[j]: first row of the contiguous run of rows ending at n-1 in column j
+    std::vector<uint32_t> run(n);
+    for (uint32_t j = 0; j < n; ++j) {
+        uint32_t a = s.sym_c_ptr[j], b = s.sym_c_ptr[j + 1];
+        if (b == a || s.sym_r_idx[b - 1] != n - 1) {
+            run[j] = n;
+            continue;
+        }
+        uint32_t p = b - 1;
+        while (p > a && s.sym_r_idx[p - 1] == s.sym_r_idx[p] - 1) --p;
+        run[j] = s.sym_r_idx[p];
+    }
+    uint32_t best = n, mx = 0;
+    for (uint32_t c = n; c-- > 0;) {
+        mx = std::max(mx, run[c]);
+        if (mx <= c)
+            best = c;
+        else
+            break;
+    }
+    t = best;
+    m = n - best;
+    if (m < min_m || m == 0) {
+        t = n;
+        m = 0;
+    }
+}
+
+uint32_t pick_group(double avg_l, uint32_t forced) {
+    if (forced) return forced;
+    if (avg_l <= 6) return 4;
+    if (avg_l <= 12) return 8;
+    if (avg_l <= 24) return 16;
+    return 32;
+}
+
+Status build_plan(glu_handle_s *h) {
+    const SymbolicData &s = h->pat;
+    const uint32_t n = h->n;
+    find_dense_tail(s, h->tune.dense_tail_min, h->t, h->m);
+    const uint32_t t = h->t, m = h->m;
+    h->doff_h.assign(std::max<uint32_t>(m, 1), 0);
+    for (uint32_t j = 0; j < m; ++j) h->doff_h[j] = s.sym_c_ptr[t + j + 1] - m;
+
+    std::vector<uint32_t> sched, item_off(1, 0);
+    h->levels_h.clear();
+    h->items_h.clear();
+    h->work_h.clear();
+    double flops = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        double L = s.sym_c_ptr[k + 1] - s.l_col_ptr[k] - 1;
+        double U = s.csr_r_ptr[k + 1] - s.csr_diag_ptr[k] - 1;
+        flops += L + 2 * L * U;
+    }
+    h->flops = flops;
+    for (int32_t l = 0; l < h->num_lev; ++l) {
+        uint32_t s0 = uint32_t(sched.size());
+        double sumL = 0;
+        uint32_t cols = 0;
+        for (int32_t q = h->level_ptr[l]; q < h->level_ptr[l + 1]; ++q) {
+            uint32_t k = uint32_t(h->level_idx[q]);
+            if (k >= t) break;  // ascending within a level
+            uint32_t L = s.sym_c_ptr[k + 1] - s.l_col_ptr[k] - 1;
+            if (L == 0) continue;
+            sched.push_back(k);
+            sumL += L;
+            ++cols;
+        }
+        if (cols == 0) continue;
+        uint32_t G = pick_group(sumL / cols, h->tune.group_lanes);
+        uint32_t CH = G * kItemUnroll;
+        uint32_t s1 = uint32_t(sched.size());
+        uint64_t items = 0, work = 0;
+        uint32_t active = 0;
+        for (uint32_t q = s0; q < s1; ++q) {
+            uint32_t k = sched[q];
+            uint64_t L = s.sym_c_ptr[k + 1] - s.l_col_ptr[k] - 1;
+            uint64_t U = s.csr_r_ptr[k + 1] - s.csr_diag_ptr[k] - 1;
+            uint64_t it = U * ((L + CH - 1) / CH);
+            items += it;
+            work += L * U;
+            if (it) ++active;
+            uint64_t next = uint64_t(item_off.back()) + it;
+            if (next > UINT32_MAX) return set_error(GLU_ERR_UNSUPPORTED, "too many work items");
+            item_off.push_back(uint32_t(next));
+        }
+        h->levels_h.push_back(LevelInfo{s0, s1, G, active > 1 ? 1u : 0u});
+        h->items_h.push_back(uint32_t(items));
+        h->work_h.push_back(work);
+    }
+    // steps: narrow runs go to the cluster kernel
+    h->steps.clear();
+    const uint32_t NL = uint32_t(h->levels_h.size());
+    uint32_t l = 0;
+    while (l < NL) {
+        if (h->work_h[l] > h->tune.wide_work || h->tune.chain_cluster == 0) {
+            h->steps.push_back(Step{STEP_LEVEL, l, l + 1});
+            ++l;
+        } else {
+            uint32_t e = l;
+            while (e < NL && h->work_h[e] <= h->tune.wide_work) ++e;
+            if (e - l == 1)
+                h->steps.push_back(Step{STEP_LEVEL, l, e});
+            else
+                h->steps.push_back(Step{STEP_CHAIN, l, e});
+            l = e;
+        }
+    }
+    GLU_CUDA(upload(h->d_sched, sched), "upload schedule");
+    GLU_CUDA(upload(h->d_item_off, item_off), "upload schedule");
+    GLU_CUDA(upload(h->d_levels, h->levels_h), "upload schedule");
+    GLU_CUDA(upload(h->d_doff, h->doff_h), "upload dense offsets");
+    h->F.sched_cols = h->d_sched.as<uint32_t>();
+    h->F.item_off = h->d_item_off.as<uint32_t>();
+    h->F.levels = h->d_levels.as<LevelInfo>();
+
+    // solve plan: dependency counts of the sparse sweeps
+    std::vector<uint32_t> lneed(n, 0), uneed(n, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t e = s.csr_r_ptr[i]; e < s.csr_diag_ptr[i]; ++e)
+            if (s.csr_c_idx[e] < t) ++lneed[i];
+        uneed[i] = s.csr_r_ptr[i + 1] - s.csr_diag_ptr[i] - 1;
+    }
+    GLU_CUDA(upload(h->d_lneed, lneed), "upload solve plan");
+    GLU_CUDA(upload(h->d_uneed, uneed), "upload solve plan");
+    h->S.t = t;
+    h->S.m = m;
+    h->S.doff = h->d_doff.as<uint32_t>();
+    h->S.l_indeg = h->d_lneed.as<uint32_t>();
+    h->S.u_indeg = h->d_uneed.as<uint32_t>();
+
+    uint32_t wide = 0, chains = 0;
+    for (auto &st : h->steps) (st.kind == STEP_CHAIN ? chains : wide)++;
+    h->stats.wide_levels = wide;
+    h->stats.chain_segments = chains;
+    h->stats.dense_tail = m;
+    h->stats.factor_flops = flops;
+    uint64_t launches = h->steps.size() + (NL ? 1 : 0) + 2;
+    if (m) launches += 2 * ((m + kDenseNB - 1) / kDenseNB);
+    h->stats.factor_launches = launches;
+    return GLU_OK;
+}
+
+Status identity_transform(glu_handle_s *h) {
+    std::vector<uint32_t> id(h->n);
+    std::iota(id.begin(), id.end(), 0u);
+    for (int k = 0; k < 4; ++k) {
+        GLU_CUDA(upload(h->d_tr[2 * k], id), "upload transform");
+        h->d_tr[2 * k + 1].release();
+    }
+    h->T = TransformDev{h->d_tr[0].as<uint32_t>(), nullptr, h->d_tr[2].as<uint32_t>(), nullptr,
+                        h->d_tr[4].as<uint32_t>(), nullptr, h->d_tr[6].as<uint32_t>(), nullptr};
+    return GLU_OK;
+}
+
+Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t *out) {
+    if (!out) return set_error(GLU_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (batch == 0) return set_error(GLU_ERR_ARG, "batch must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_error(GLU_ERR_NO_DEVICE, "no CUDA device available");
+    if (device < 0 || device >= ndev) return set_error(GLU_ERR_ARG, "device %d out of range", device);
+    DeviceGuard g(device);
+    std::unique_ptr<glu_handle_s> h(new glu_handle_s());
+    h->device = device;
+    h->n = s.n;
+    h->nnz = s.nnz;
+    h->batch = batch;
+    h->pat = std::move(s);
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 1.0f};
+    const SymbolicData &p = h->pat;
+    GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
+    GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
+    GLU_CUDA(upload(h->d_diag, p.l_col_ptr), "upload pattern");
+    GLU_CUDA(upload(h->d_rptr, p.csr_r_ptr), "upload pattern");
+    GLU_CUDA(upload(h->d_cidx, p.csr_c_idx), "upload pattern");
+    GLU_CUDA(upload(h->d_rdiag, p.csr_diag_ptr), "upload pattern");
+    GLU_CUDA(upload(h->d_cpos, p.csr_pos), "upload pattern");
+    h->P = DevPattern{h->d_cptr.as<uint32_t>(), h->d_ridx.as<uint32_t>(), h->d_diag.as<uint32_t>(),
+                      h->d_rptr.as<uint32_t>(), h->d_cidx.as<uint32_t>(), h->d_rdiag.as<uint32_t>(),
+                      h->d_cpos.as<uint32_t>(), h->n, h->nnz};
+    GLU_CUDA(h->d_val.alloc(sizeof(float) * size_t(h->nnz) * batch), "allocate values");
+    GLU_CUDA(cudaMemset(h->d_val.p, 0, sizeof(float) * size_t(h->nnz) * batch), "clear values");
+    GLU_CUDA(h->d_status.alloc(256), "allocate status");
+    GLU_CUDA(cudaMemset(h->d_status.p, 0, 256), "clear status");
+    GLU_CUDA(h->d_pert.alloc(sizeof(float) * batch), "allocate");
+    GLU_CUDA(h->d_colmax.alloc(sizeof(float) * batch), "allocate");
+    GLU_CUDA(h->d_diag_scratch.alloc(sizeof(float) * kDenseNB * kDenseNB * batch), "allocate");
+    GLU_CUDA(h->d_counters.alloc(sizeof(uint32_t) * (size_t(h->n) + 64)), "allocate");
+    GLU_CUDA(h->d_ticket.alloc(256), "allocate");
+    GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_status), 256), "allocate pinned");
+    GLU_CUDA(cudaEventCreate(&h->ev0), "event");
+    GLU_CUDA(cudaEventCreate(&h->ev1), "event");
+
+    // level sets on the device
+    {
+        DevBuf scratch, level_of, lptr, lidx, nlev;
+        GLU_CUDA(scratch.alloc(level_scratch_bytes(h->n)), "allocate level scratch");
+        GLU_CUDA(level_of.alloc(sizeof(int32_t) * h->n), "allocate levels");
+        GLU_CUDA(lptr.alloc(sizeof(int32_t) * (size_t(h->n) + 1)), "allocate levels");
+        GLU_CUDA(lidx.alloc(sizeof(int32_t) * h->n), "allocate levels");
+        GLU_CUDA(nlev.alloc(sizeof(int32_t)), "allocate levels");
+        GLU_CUDA(build_levels(h->P, scratch.p, level_of.as<int32_t>(), lptr.as<int32_t>(),
+                              lidx.as<int32_t>(), nlev.as<int32_t>(), h->d_status.as<uint32_t>(), 0),
+                 "build levels");
+        GLU_CUDA(cudaMemcpy(&h->num_lev, nlev.p, sizeof(int32_t), cudaMemcpyDeviceToHost), "levels");
+        uint32_t st = 0;
+        GLU_CUDA(cudaMemcpy(&st, h->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost), "levels");
+        if (st & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "level construction wait timed out");
+        h->level_ptr.resize(size_t(h->num_lev) + 1);
+        h->level_idx.resize(h->n);
+        GLU_CUDA(cudaMemcpy(h->level_ptr.data(), lptr.p, sizeof(int32_t) * h->level_ptr.size(),
+                            cudaMemcpyDeviceToHost), "levels");
+        GLU_CUDA(cudaMemcpy(h->level_idx.data(), lidx.p, sizeof(int32_t) * h->n, cudaMemcpyDeviceToHost),
+                 "levels");
+    }
+    int maxc = 0;
+    h->chain_cluster = 16;
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(16, 1, 1);
+        cfg.blockDim = dim3(kChainThreads, 1, 1);
+        cudaLaunchAttribute a[1];
+        a[0].id = cudaLaunchAttributeClusterDimension;
+        a[0].val.clusterDim.x = 16;
+        a[0].val.clusterDim.y = 1;
+        a[0].val.clusterDim.z = 1;
+        cfg.attrs = a;
+        cfg.numAttrs = 1;
+        cudaFuncSetAttribute(chain_kernel_ptr(), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (cudaOccupancyMaxActiveClusters(&maxc, chain_kernel_ptr(), &cfg) != cudaSuccess || maxc < 1)
+            h->chain_cluster = 8;
+        cudaGetLastError();
+    }
+    h->tune.chain_cluster = h->chain_cluster;
+    Status st = build_plan(h.get());
+    if (st != GLU_OK) return st;
+    st = identity_transform(h.get());
+    if (st != GLU_OK) return st;
+    h->stats.n = h->n;
+    h->stats.nnz_lu = h->nnz;
+    h->stats.batch = batch;
+    h->stats.num_lev = h->num_lev;
+    *out = h.release();
+    return GLU_OK;
+}
+
+Status check_range(glu_handle_s *h, uint32_t first, uint32_t count) {
+    if (count == 0 || first >= h->batch || count > h->batch - first)
+        return set_error(GLU_ERR_ARG, "value sets [%u, %u) outside batch %u", first, first + count, h->batch);
+    return GLU_OK;
+}
+
+Status read_status(glu_handle_s *h, cudaStream_t st, uint32_t *flags) {
+    GLU_CUDA(cudaMemcpyAsync(h->h_status, h->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+             "read status");
+    GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
+    *flags = h->h_status[0];
+    return GLU_OK;
+}
+
+// One FP32 solve of y in place (nrhs vectors of n), in the permuted system.
+Status solve_inplace(glu_handle_s *h, const float *val, float *y, uint32_t nrhs, bool trans, cudaStream_t st) {
+    uint32_t *cnt = h->d_counters.as<uint32_t>();
+    uint32_t *tk = h->d_ticket.as<uint32_t>();
+    uint32_t *status = h->d_status.as<uint32_t>();
+    if (!trans) {
+        GLU_CUDA(solve_lower_unit(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "lower solve");
+        GLU_CUDA(solve_upper(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "upper solve");
+    } else {
+        GLU_CUDA(solve_upper_trans(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "transposed upper solve");
+        GLU_CUDA(solve_lower_unit_trans(h->P, h->S, val, y, nrhs, cnt, tk, status, st),
+                 "transposed lower solve");
+    }
+    return GLU_OK;
+}
+
+Status solve_f32(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
+                 glu_memory where, bool trans, cudaStream_t st) {
+    if (!h->factored) return set_error(GLU_ERR_STATE, "solve before factorization");
+    if (inst >= h->batch) return set_error(GLU_ERR_ARG, "value set %u outside batch", inst);
+    if (nrhs == 0) return GLU_OK;
+    if (!b || !x) return set_error(GLU_ERR_ARG, "null vector");
+    DeviceGuard g(h->device);
+    const size_t len = size_t(h->n) * nrhs;
+    GLU_CUDA(h->d_y.ensure(sizeof(float) * len), "allocate solve buffer");
+    GLU_CUDA(h->d_io32.ensure(sizeof(float) * len), "allocate solve buffer");
+    float *y = h->d_y.as<float>();
+    float *io = h->d_io32.as<float>();
+    const float *bin = b;
+    if (where == GLU_HOST) {
+        GLU_CUDA(cudaMemcpyAsync(io, b, sizeof(float) * len, cudaMemcpyHostToDevice, st), "copy b");
+        bin = io;
+    }
+    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
+    const TransformDev &T = h->T;
+    GLU_CUDA(launch_transform_f32(trans ? T.tin_idx : T.in_idx, trans ? T.tin_scale : T.in_scale, bin, y,
+                                  h->n, nrhs, st), "transform");
+    const float *val = h->d_val.as<float>() + size_t(inst) * h->nnz;
+    Status s = solve_inplace(h, val, y, nrhs, trans, st);
+    if (s != GLU_OK) return s;
+    float *xout = (where == GLU_HOST) ? io : x;
+    GLU_CUDA(launch_transform_f32(trans ? T.tout_idx : T.out_idx, trans ? T.tout_scale : T.out_scale, y,
+                                  xout, h->n, nrhs, st), "transform");
+    if (where == GLU_HOST)
+        GLU_CUDA(cudaMemcpyAsync(x, io, sizeof(float) * len, cudaMemcpyDeviceToHost, st), "copy x");
+    uint32_t flags = 0;
+    s = read_status(h, st, &flags);
+    if (s != GLU_OK) return s;
+    if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
+    return GLU_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI ==
+extern "C" {
+
+const char *glu_last_error(void) { return g_last_error.c_str(); }
+const char *glu_version(void) { return "glu_b200 0.1 (sm_100a)"; }
+
+glu_status glu_symbolic_analyze(uint32_t n, uint32_t nnz_a, const uint32_t *ap, const uint32_t *ai,
+                                glu_symbolic_t *out) {
+    if (!out || !ap || (nnz_a && !ai)) return set_error(GLU_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::unique_ptr<glu_symbolic_s> s(new glu_symbolic_s());
+    Status st = symbolic_analyze(n, nnz_a, ap, ai, s->s);
+    if (st != GLU_OK) return st;
+    *out = s.release();
+    return GLU_OK;
+}
+
+glu_status glu_symbolic_sizes(glu_symbolic_t s, uint32_t *n, uint32_t *nnz_lu) {
+    if (!s) return set_error(GLU_ERR_ARG, "null symbolic handle");
+    if (n) *n = s->s.n;
+    if (nnz_lu) *nnz_lu = s->s.nnz;
+    return GLU_OK;
+}
+
+glu_status glu_symbolic_export(glu_symbolic_t s, uint32_t *sym_c_ptr, uint32_t *sym_r_idx,
+                               uint32_t *l_col_ptr, uint32_t *csr_r_ptr, uint32_t *csr_c_idx,
+                               uint32_t *csr_diag_ptr) {
+    if (!s) return set_error(GLU_ERR_ARG, "null symbolic handle");
+    const SymbolicData &d = s->s;
+    auto cp = [](uint32_t *dst, const std::vector<uint32_t> &v) {
+        if (dst && !v.empty()) memcpy(dst, v.data(), sizeof(uint32_t) * v.size());
+    };
+    cp(sym_c_ptr, d.sym_c_ptr);
+    cp(sym_r_idx, d.sym_r_idx);
+    cp(l_col_ptr, d.l_col_ptr);
+    cp(csr_r_ptr, d.csr_r_ptr);
+    cp(csr_c_idx, d.csr_c_idx);
+    cp(csr_diag_ptr, d.csr_diag_ptr);
+    return GLU_OK;
+}
+
+glu_status glu_symbolic_slots(glu_symbolic_t s, uint32_t *a_slot) {
+    if (!s || !a_slot) return set_error(GLU_ERR_ARG, "null argument");
+    if (!s->s.a_slot.empty()) memcpy(a_slot, s->s.a_slot.data(), sizeof(uint32_t) * s->s.a_slot.size());
+    return GLU_OK;
+}
+
+glu_status glu_predict_lu(glu_symbolic_t s, const double *ax, float *val) {
+    if (!s || !val || (s->s.nnz_a && !ax)) return set_error(GLU_ERR_ARG, "null argument");
+    predict_lu(s->s, ax, val);
+    return GLU_OK;
+}
+
+void glu_symbolic_destroy(glu_symbolic_t s) { delete s; }
+
+glu_status glu_create(glu_symbolic_t s, int device, uint32_t batch, glu_handle_t *out) {
+    if (!s) return set_error(GLU_ERR_ARG, "null symbolic handle");
+    SymbolicData copy = s->s;
+    return create_handle(device, std::move(copy), batch, out);
+}
+
+glu_status glu_create_from_pattern(int device, uint32_t n, uint32_t nnz, const uint32_t *sym_c_ptr,
+                                   const uint32_t *sym_r_idx, const uint32_t *l_col_ptr,
+                                   const uint32_t *csr_r_ptr, const uint32_t *csr_c_idx,
+                                   const uint32_t *csr_diag_ptr, uint32_t batch, glu_handle_t *out) {
+    if (!sym_c_ptr || !sym_r_idx || !l_col_ptr || !csr_r_ptr || !csr_c_idx || !csr_diag_ptr)
+        return set_error(GLU_ERR_ARG, "null pattern array");
+    if (n == 0 || sym_c_ptr[0] != 0 || sym_c_ptr[n] != nnz || csr_r_ptr[n] != nnz)
+        return set_error(GLU_ERR_ARG, "inconsistent pattern");
+    SymbolicData s;
+    s.n = n;
+    s.nnz = nnz;
+    s.sym_c_ptr.assign(sym_c_ptr, sym_c_ptr + n + 1);
+    s.sym_r_idx.assign(sym_r_idx, sym_r_idx + nnz);
+    s.l_col_ptr.assign(l_col_ptr, l_col_ptr + n);
+    s.csr_r_ptr.assign(csr_r_ptr, csr_r_ptr + n + 1);
+    s.csr_c_idx.assign(csr_c_idx, csr_c_idx + nnz);
+    s.csr_diag_ptr.assign(csr_diag_ptr, csr_diag_ptr + n);
+    for (uint32_t i = 0; i < n; ++i) {
+        if (sym_c_ptr[i] > sym_c_ptr[i + 1] || l_col_ptr[i] < sym_c_ptr[i] || l_col_ptr[i] >= sym_c_ptr[i + 1] ||
+            sym_r_idx[l_col_ptr[i]] != i)
+            return set_error(GLU_ERR_ARG, "invalid diagonal pointer of column %u", i);
+    }
+    for (uint32_t p = 0; p < nnz; ++p)
+        if (sym_r_idx[p] >= n) return set_error(GLU_ERR_ARG, "row index out of range");
+    // CSC positions of the CSR entries (rows ascending in every column)
+    s.csr_pos.resize(nnz);
+    {
+        std::vector<uint32_t> fillp(s.csr_r_ptr.begin(), s.csr_r_ptr.end() - 1);
+        for (uint32_t c = 0; c < n; ++c)
+            for (uint32_t p = s.sym_c_ptr[c]; p < s.sym_c_ptr[c + 1]; ++p) {
+                uint32_t r = s.sym_r_idx[p];
+                uint32_t e = fillp[r]++;
+                if (e >= s.csr_r_ptr[r + 1] || s.csr_c_idx[e] != c)
+                    return set_error(GLU_ERR_ARG, "CSR arrays do not transpose the CSC pattern");
+                s.csr_pos[e] = p;
+            }
+    }
+    return create_handle(device, std::move(s), batch, out);
+}
+
+void glu_destroy(glu_handle_t h) {
+    if (!h) return;
+    DeviceGuard g(h->device);
+    delete h;
+}
+
+glu_status glu_levels(glu_handle_t h, int32_t *num_lev, int32_t *level_ptr, int32_t *level_idx) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    if (num_lev) *num_lev = h->num_lev;
+    if (level_ptr) memcpy(level_ptr, h->level_ptr.data(), sizeof(int32_t) * h->level_ptr.size());
+    if (level_idx) memcpy(level_idx, h->level_idx.data(), sizeof(int32_t) * h->level_idx.size());
+    return GLU_OK;
+}
+
+glu_status glu_set_transform(glu_handle_t h, const uint32_t *col_perm, const uint32_t *row_perm_inv,
+                             const int32_t *pivot, const double *col_scale_perm, const double *row_scale,
+                             int mc64_scale) {
+    if (!h || !col_perm || !row_perm_inv || !pivot) return set_error(GLU_ERR_ARG, "null argument");
+    if (mc64_scale && (!col_scale_perm || !row_scale)) return set_error(GLU_ERR_ARG, "null scale array");
+    const uint32_t n = h->n;
+    std::vector<uint32_t> in_idx(n), out_idx(n), tin_idx(n), tout_idx(n);
+    std::vector<double> in_s(n), out_s(n), tin_s(n), tout_s(n);
+    std::vector<uint32_t> cp_inv(n, UINT32_MAX), g(n, UINT32_MAX);
+    for (uint32_t j = 0; j < n; ++j) {
+        int32_t pj = pivot[j];
+        if (pj < 0 || uint32_t(pj) >= n || col_perm[pj] >= n || row_perm_inv[j] >= n)
+            return set_error(GLU_ERR_ARG, "permutation entry out of range");
+        in_idx[j] = col_perm[pj];  // b[j] = rhs[rp[piv[j]]] * rows[piv[j]]
+        in_s[j] = mc64_scale ? col_scale_perm[pj] : 1.0;
+        out_idx[j] = row_perm_inv[j];  // x[j] = b[cp[j]] * cols[j]
+        out_s[j] = mc64_scale ? row_scale[j] : 1.0;
+        if (cp_inv[row_perm_inv[j]] != UINT32_MAX || g[in_idx[j]] != UINT32_MAX)
+            return set_error(GLU_ERR_ARG, "permutation is not one-to-one");
+        cp_inv[row_perm_inv[j]] = j;
+        g[in_idx[j]] = j;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        tin_idx[i] = cp_inv[i];  // A^T: y[cp[j]] = b[j] * cols[j]
+        tin_s[i] = out_s[cp_inv[i]];
+        tout_idx[i] = g[i];  // x[rp[piv[j]]] = z[j] * rows[piv[j]]
+        tout_s[i] = in_s[g[i]];
+    }
+    DeviceGuard gd(h->device);
+    GLU_CUDA(upload(h->d_tr[0], in_idx), "upload transform");
+    GLU_CUDA(upload(h->d_tr[2], out_idx), "upload transform");
+    GLU_CUDA(upload(h->d_tr[4], tin_idx), "upload transform");
+    GLU_CUDA(upload(h->d_tr[6], tout_idx), "upload transform");
+    if (mc64_scale) {
+        GLU_CUDA(upload(h->d_tr[1], in_s), "upload transform");
+        GLU_CUDA(upload(h->d_tr[3], out_s), "upload transform");
+        GLU_CUDA(upload(h->d_tr[5], tin_s), "upload transform");
+        GLU_CUDA(upload(h->d_tr[7], tout_s), "upload transform");
+    } else {
+        for (int k = 1; k < 8; k += 2) h->d_tr[k].release();
+    }
+    h->T = TransformDev{h->d_tr[0].as<uint32_t>(), h->d_tr[1].as<double>(), h->d_tr[2].as<uint32_t>(),
+                        h->d_tr[3].as<double>(),   h->d_tr[4].as<uint32_t>(), h->d_tr[5].as<double>(),
+                        h->d_tr[6].as<uint32_t>(), h->d_tr[7].as<double>()};
+    h->has_transform = true;
+    return GLU_OK;
+}
+
+glu_status glu_set_source(glu_handle_t h, uint32_t nnz_src, const uint32_t *src_ap, const uint32_t *src_ai,
+                          const uint32_t *src_slot, const double *src_scale) {
+    if (!h || !src_ap || (nnz_src && (!src_ai || !src_slot))) return set_error(GLU_ERR_ARG, "null argument");
+    const uint32_t n = h->n;
+    if (src_ap[0] != 0 || src_ap[n] != nnz_src) return set_error(GLU_ERR_ARG, "inconsistent source pointers");
+    std::vector<int64_t> lu_src(h->nnz, -1);
+    std::vector<uint32_t> rcount(n + 1, 0);
+    for (uint32_t c = 0; c < n; ++c) {
+        if (src_ap[c] > src_ap[c + 1]) return set_error(GLU_ERR_ARG, "source pointers not monotone");
+        for (uint32_t q = src_ap[c]; q < src_ap[c + 1]; ++q) {
+            if (src_ai[q] >= n || src_slot[q] >= h->nnz) return set_error(GLU_ERR_ARG, "source entry out of range");
+            if (lu_src[src_slot[q]] < 0) lu_src[src_slot[q]] = int64_t(q);
+            rcount[src_ai[q] + 1]++;
+        }
+    }
+    // CSR of A0 for the FP64 residual
+    for (uint32_t r = 0; r < n; ++r) rcount[r + 1] += rcount[r];
+    std::vector<uint32_t> rptr(rcount), cidx(nnz_src), vmap(nnz_src), ident(nnz_src);
+    {
+        std::vector<uint32_t> fillp(rcount.begin(), rcount.end() - 1);
+        for (uint32_t c = 0; c < n; ++c)
+            for (uint32_t q = src_ap[c]; q < src_ap[c + 1]; ++q) {
+                uint32_t e = fillp[src_ai[q]]++;
+                cidx[e] = c;
+                vmap[e] = q;
+            }
+    }
+    std::iota(ident.begin(), ident.end(), 0u);
+    std::vector<double> scale(nnz_src, 1.0);
+    if (src_scale) scale.assign(src_scale, src_scale + nnz_src);
+    DeviceGuard g(h->device);
+    GLU_CUDA(upload(h->d_src_lu, lu_src), "upload source");
+    GLU_CUDA(upload(h->d_src_scale, scale), "upload source");
+    GLU_CUDA(upload(h->d_a0_rptr, rptr), "upload source");
+    GLU_CUDA(upload(h->d_a0_cidx, cidx), "upload source");
+    GLU_CUDA(upload(h->d_a0_vmap, vmap), "upload source");
+    GLU_CUDA(upload(h->d_a0_cptr, std::vector<uint32_t>(src_ap, src_ap + n + 1)), "upload source");
+    GLU_CUDA(upload(h->d_a0_ridx, std::vector<uint32_t>(src_ai, src_ai + nnz_src)), "upload source");
+    GLU_CUDA(upload(h->d_a0_ident, ident), "upload source");
+    GLU_CUDA(h->d_ax0.alloc(sizeof(double) * std::max<size_t>(size_t(nnz_src) * h->batch, 1)), "allocate source values");
+    h->nnz_src = nnz_src;
+    h->has_source = true;
+    h->ax0_loaded = false;
+    return GLU_OK;
+}
+
+glu_status glu_load_lu_values(glu_handle_t h, uint32_t first, uint32_t count, const float *val,
+                              glu_memory where, glu_stream stream) {
+    if (!h || !val) return set_error(GLU_ERR_ARG, "null argument");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    DeviceGuard g(h->device);
+    GLU_CUDA(cudaMemcpyAsync(h->d_val.as<float>() + size_t(first) * h->nnz, val,
+                             sizeof(float) * size_t(h->nnz) * count,
+                             where == GLU_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, S_(stream)),
+             "copy values");
+    if (where == GLU_HOST) GLU_CUDA(cudaStreamSynchronize(S_(stream)), "synchronize");
+    h->factored = false;
+    return GLU_OK;
+}
+
+glu_status glu_store_lu_values(glu_handle_t h, uint32_t first, uint32_t count, float *val,
+                               glu_memory where, glu_stream stream) {
+    if (!h || !val) return set_error(GLU_ERR_ARG, "null argument");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    DeviceGuard g(h->device);
+    GLU_CUDA(cudaMemcpyAsync(val, h->d_val.as<float>() + size_t(first) * h->nnz,
+                             sizeof(float) * size_t(h->nnz) * count,
+                             where == GLU_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, S_(stream)),
+             "copy values");
+    if (where == GLU_HOST) GLU_CUDA(cudaStreamSynchronize(S_(stream)), "synchronize");
+    return GLU_OK;
+}
+
+glu_status glu_load_source_values(glu_handle_t h, uint32_t first, uint32_t count, const double *ax0,
+                                  glu_memory where, glu_stream stream) {
+    if (!h || !ax0) return set_error(GLU_ERR_ARG, "null argument");
+    if (!h->has_source) return set_error(GLU_ERR_STATE, "no source matrix set (glu_set_source)");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    DeviceGuard g(h->device);
+    cudaStream_t st = S_(stream);
+    double *dst = h->d_ax0.as<double>() + size_t(first) * h->nnz_src;
+    GLU_CUDA(cudaMemcpyAsync(dst, ax0, sizeof(double) * size_t(h->nnz_src) * count,
+                             where == GLU_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
+             "copy source values");
+    GLU_CUDA(launch_gather_values(h->d_src_lu.as<int64_t>(), dst, h->nnz_src, h->d_src_scale.as<double>(),
+                                  h->nnz, h->d_val.as<float>() + size_t(first) * h->nnz, h->nnz, count, st),
+             "place values");
+    if (where == GLU_HOST) GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
+    h->ax0_loaded = true;
+    h->factored = false;
+    return GLU_OK;
+}
+
+glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int perturb, glu_stream stream) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    DeviceGuard g(h->device);
+    cudaStream_t st = S_(stream);
+    float *val = h->d_val.as<float>() + size_t(first) * h->nnz;
+    const uint64_t stride = h->nnz;
+    const float *pert = nullptr;
+    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
+    GLU_CUDA(cudaEventRecord(h->ev0, st), "event");
+    if (perturb) {
+        GLU_CUDA(launch_pert(h->P, val, stride, count, h->d_colmax.as<float>(),
+                             h->d_pert.as<float>() + first, st), "perturbation");
+        pert = h->d_pert.as<float>() + first;
+    }
+    const uint32_t NL = uint32_t(h->levels_h.size());
+    for (const Step &stp : h->steps) {
+        if (stp.kind == STEP_CHAIN) {
+            GLU_CUDA(launch_factor_chain(h->P, h->F, val, stride, count, pert, stp.l0, stp.l1, h->chain_cluster, st),
+                     "factor (narrow levels)");
+        } else {
+            const LevelInfo &cur = h->levels_h[stp.l0];
+            const LevelInfo *prev = stp.l0 > 0 ? &h->levels_h[stp.l0 - 1] : nullptr;
+            GLU_CUDA(launch_factor_level(h->P, h->F, val, stride, count, pert, cur, prev, h->items_h[stp.l0], st),
+                     "factor (level)");
+        }
+    }
+    if (NL) GLU_CUDA(launch_scale_level(h->P, h->F, val, stride, count, pert, h->levels_h[NL - 1], st), "factor (scale)");
+    for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
+        uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
+        uint32_t last_has_l = 0;  // the last column of the matrix has no L part
+        GLU_CUDA(launch_dense_panel(val, stride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
+                                    h->d_diag_scratch.as<float>(), last_has_l, st), "factor (dense panel)");
+        GLU_CUDA(launch_dense_update(val, stride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
+                                     h->d_diag_scratch.as<float>(), st), "factor (dense update)");
+    }
+    GLU_CUDA(launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
+    GLU_CUDA(cudaEventRecord(h->ev1, st), "event");
+    uint32_t flags = 0;
+    s = read_status(h, st, &flags);
+    if (s != GLU_OK) return s;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.last_factor_ms = ms;
+    if (perturb) cudaMemcpy(&h->stats.pert, h->d_pert.as<float>() + first, sizeof(float), cudaMemcpyDeviceToHost);
+    h->factored = true;
+    if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "factorization wait timed out");
+    if (flags & (DEV_ZERO_PIVOT | DEV_NONFINITE_PIVOT))
+        return set_error(GLU_ERR_SINGULAR, "%s pivot encountered", (flags & DEV_ZERO_PIVOT) ? "zero" : "non-finite");
+    return GLU_OK;
+}
+
+glu_status glu_solve(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
+                     glu_memory where, glu_stream stream) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    return solve_f32(h, inst, nrhs, b, x, where, false, S_(stream));
+}
+
+glu_status glu_solve_transposed(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
+                                glu_memory where, glu_stream stream) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    return solve_f32(h, inst, nrhs, b, x, where, true, S_(stream));
+}
+
+glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uint32_t nrhs,
+                             const double *b, double *x, double tol, uint32_t maxit, int transposed,
+                             glu_memory where, glu_refine_stats *stats, glu_stream stream) {
+    if (!h || !b || !x) return set_error(GLU_ERR_ARG, "null argument");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    if (!h->factored) return set_error(GLU_ERR_STATE, "solve before factorization");
+    if (!h->has_source || !h->ax0_loaded)
+        return set_error(GLU_ERR_STATE, "refinement needs the source matrix values (glu_load_source_values)");
+    if (nrhs == 0) return GLU_OK;
+    DeviceGuard g(h->device);
+    cudaStream_t st = S_(stream);
+    const uint32_t n = h->n;
+    const size_t len = size_t(n) * nrhs;
+    GLU_CUDA(h->d_y.ensure(sizeof(float) * len), "allocate");
+    GLU_CUDA(h->d_b64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
+    GLU_CUDA(h->d_x64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
+    GLU_CUDA(h->d_r64.ensure(sizeof(double) * len), "allocate");
+    GLU_CUDA(h->d_norms.ensure(sizeof(double) * 4 * nrhs), "allocate");
+    if (h->h_norms_cap < 4 * size_t(nrhs)) {
+        if (h->h_norms) cudaFreeHost(h->h_norms);
+        h->h_norms = nullptr;
+        GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_norms), sizeof(double) * 4 * nrhs), "allocate pinned");
+        h->h_norms_cap = 4 * size_t(nrhs);
+    }
+    const TransformDev &T = h->T;
+    const bool tr = transposed != 0;
+    const uint32_t *in_idx = tr ? T.tin_idx : T.in_idx;
+    const double *in_s = tr ? T.tin_scale : T.in_scale;
+    const uint32_t *out_idx = tr ? T.tout_idx : T.out_idx;
+    const double *out_s = tr ? T.tout_scale : T.out_scale;
+    const uint32_t *rptr = tr ? h->d_a0_cptr.as<uint32_t>() : h->d_a0_rptr.as<uint32_t>();
+    const uint32_t *cidx = tr ? h->d_a0_ridx.as<uint32_t>() : h->d_a0_cidx.as<uint32_t>();
+    const uint32_t *vmap = tr ? h->d_a0_ident.as<uint32_t>() : h->d_a0_vmap.as<uint32_t>();
+    glu_refine_stats agg{0, 0.0, 0.0};
+    bool converged_all = true;
+    float *y = h->d_y.as<float>();
+    double *r = h->d_r64.as<double>();
+    double *norms = h->d_norms.as<double>();
+    for (uint32_t z = first; z < first + count; ++z) {
+        const size_t off = size_t(z - first) * len;
+        const double *bz;
+        double *xz;
+        if (where == GLU_HOST) {
+            GLU_CUDA(cudaMemcpyAsync(h->d_b64.p, b + off, sizeof(double) * len, cudaMemcpyHostToDevice, st), "copy b");
+            bz = h->d_b64.as<double>();
+            xz = h->d_x64.as<double>();
+        } else {
+            bz = b + off;
+            xz = x + off;
+        }
+        const float *val = h->d_val.as<float>() + size_t(z) * h->nnz;
+        const double *ax0 = h->d_ax0.as<double>() + size_t(z) * h->nnz_src;
+        GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
+        GLU_CUDA(launch_norms(bz, n, nrhs, norms + 2 * nrhs, st), "norms");
+        // x0 = solve(b)
+        GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, bz, y, n, nrhs, st), "transform");
+        s = solve_inplace(h, val, y, nrhs, tr, st);
+        if (s != GLU_OK) return s;
+        GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 0, st), "transform");
+        uint32_t it = 0;
+        double worst2 = 0, worstinf = 0;
+        for (;; ++it) {
+            GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, n, bz, xz, r, nrhs, norms, st), "residual");
+            GLU_CUDA(cudaMemcpyAsync(h->h_norms, norms, sizeof(double) * 4 * nrhs, cudaMemcpyDeviceToHost, st),
+                     "read norms");
+            GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
+            worst2 = 0;
+            worstinf = 0;
+            for (uint32_t v = 0; v < nrhs; ++v) {
+                double bn2 = std::sqrt(h->h_norms[2 * nrhs + 2 * v]), bninf = h->h_norms[2 * nrhs + 2 * v + 1];
+                double rn2 = std::sqrt(h->h_norms[2 * v]), rninf = h->h_norms[2 * v + 1];
+                double rel2 = bn2 > 0 ? rn2 / bn2 : rn2, relinf = bninf > 0 ? rninf / bninf : rninf;
+                if (!(rel2 == rel2)) rel2 = INFINITY;
+                worst2 = std::max(worst2, rel2);
+                worstinf = std::max(worstinf, relinf);
+            }
+            if (worst2 <= tol || it >= maxit) break;
+            GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, r, y, n, nrhs, st), "transform");
+            s = solve_inplace(h, val, y, nrhs, tr, st);
+            if (s != GLU_OK) return s;
+            GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 1, st), "transform");
+        }
+        if (where == GLU_HOST)
+            GLU_CUDA(cudaMemcpyAsync(x + off, xz, sizeof(double) * len, cudaMemcpyDeviceToHost, st), "copy x");
+        uint32_t flags = 0;
+        s = read_status(h, st, &flags);
+        if (s != GLU_OK) return s;
+        if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
+        agg.iterations = std::max(agg.iterations, it);
+        agg.residual = std::max(agg.residual, worst2);
+        agg.residual_inf = std::max(agg.residual_inf, worstinf);
+        if (!(worst2 <= tol)) converged_all = false;
+    }
+    if (stats) *stats = agg;
+    if (!converged_all)
+        return set_error(GLU_ERR_NOT_CONVERGED, "refinement stopped at relative residual %.3e > %.3e",
+                         agg.residual, tol);
+    return GLU_OK;
+}
+
+glu_status glu_get_stats(glu_handle_t h, glu_stats *stats) {
+    if (!h || !stats) return set_error(GLU_ERR_ARG, "null argument");
+    *stats = h->stats;
+    return GLU_OK;
+}
+
+glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t) {
+    if (!h || !t) return set_error(GLU_ERR_ARG, "null argument");
+    *t = h->tune;
+    return GLU_OK;
+}
+
+glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t) {
+    if (!h || !t) return set_error(GLU_ERR_ARG, "null argument");
+    if (t->group_lanes && (t->group_lanes < 4 || t->group_lanes > 32 || (t->group_lanes & (t->group_lanes - 1))))
+        return set_error(GLU_ERR_ARG, "group_lanes must be 0 or a power of two in [4, 32]");
+    if (t->chain_cluster > 16) return set_error(GLU_ERR_ARG, "chain_cluster must be <= 16");
+    DeviceGuard g(h->device);
+    h->tune = *t;
+    if (h->tune.chain_cluster) h->chain_cluster = h->tune.chain_cluster;
+    Status s = build_plan(h);
+    h->factored = false;
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,330 @@
+// Dense trailing block of the numeric factorization, factored in place.
+//
+// The circuit and grid matrices this engine targets end in a trailing block
+// [t, n) x [t, n) in which every entry is in the L+U pattern.  In the CSC
+// layout the rows t..n-1 of each such column are its last m = n - t entries,
+// so the block is a column-major matrix with one base offset per column
+// (element (i, j) at val[doff[j] + i]) and can be factored where it lies,
+// without a copy.  The right-looking column algorithm of the reference
+// (src/numeric.cu:10-345) applied to this block is the unpivoted dense LU; it
+// is computed here blocked (panel width kDenseNB):
+//   1. panel:  A11 = L11 U11 (every block factors the small diagonal block in
+//              shared memory), L21 = A21 U11^-1, U12 = L11^-1 A12;
+//   2. update: A22 -= L21 U12 (register-tiled FP32).
+// Each entry receives the same operations as in the column algorithm (FP32,
+// different summation order).  GESP perturbation (numeric.cu:139-140) is
+// applied to every pivot whose column has an L part.
+#include "glu_common.cuh"
+#include "glu_kernels.h"
+
+namespace glu {
+
+// Factor the kb x kb diagonal block at (k0, k0) of the dense block in shared
+// memory sF (column-major, leading dimension kDenseNB+1).  Step c: the pivot
+// is fixed (GESP), every row i > c computes L(i,c) = A(i,c) / d once, then the
+// block's threads update A(i,j), j > c, with a row split into halves between
+// two threads.  Returns with sF holding L11 (unit, strictly lower) and U11.
+__device__ __forceinline__ void factor_diag_block(const float *__restrict__ val,
+                                                  const uint32_t *__restrict__ doff, uint32_t k0,
+                                                  uint32_t kb, uint32_t m, float pert,
+                                                  uint32_t last_has_l, float *sF, float *lcol) {
+    constexpr int LD = kDenseNB + 1;
+    const uint32_t tid = threadIdx.x;
+    // load: consecutive threads take consecutive rows of a column
+    for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
+        uint32_t j = e / kb, i = e - j * kb;
+        sF[j * LD + i] = ld_cg(val + doff[k0 + j] + k0 + i);
+    }
+    __syncthreads();
+    const uint32_t row = tid >> 1, half = tid & 1;  // 64 rows x 2 halves
+    for (uint32_t c = 0; c < kb; ++c) {
+        // a pivot is perturbed only when its column has an L part
+        const bool has_l = (k0 + c + 1 < m) || last_has_l;
+        const float d = sF[c * LD + c];
+        const float de = (has_l && pert > 0.0f && fabsf(d) < pert) ? pert : d;
+        if (half == 0 && row > c && row < kb) {
+            float l = sF[c * LD + row] / de;
+            sF[c * LD + row] = l;
+            lcol[row] = l;
+        }
+        // (a concurrent reader sees d or pert; both give the same de)
+        if (tid == 0 && de != d) sF[c * LD + c] = de;
+        __syncthreads();
+        if (row > c && row < kb) {
+            const float l = lcol[row];
+            for (uint32_t j = c + 1 + half; j < kb; j += 2) sF[j * LD + row] -= l * sF[j * LD + c];
+        }
+        __syncthreads();
+    }
+}
+
+// Panel step.  Block 0 stores the factored diagonal block to diag_scratch (the
+// update kernel writes it back, so no block here overwrites an entry another
+// block may still read); blocks [1, 1+nL) compute rows of L21, the rest
+// columns of U12.  blockIdx.z selects the value set.
+__global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uint64_t stride,
+                                                            const uint32_t *__restrict__ doff,
+                                                            uint32_t m, uint32_t k0, uint32_t kb,
+                                                            const float *pert_z, float *diag_scratch,
+                                                            uint32_t last_has_l, uint32_t nL) {
+    constexpr int NB = kDenseNB;
+    constexpr int LD = kDenseNB + 1;
+    __shared__ float sF[NB * LD];
+    __shared__ float lcol[NB];
+    float *val = val_base + blockIdx.z * stride;
+    float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
+    factor_diag_block(val, doff, k0, kb, m, pert, last_has_l, sF, lcol);
+    const uint32_t r0 = k0 + kb;
+    const uint32_t tid = threadIdx.x;
+    if (blockIdx.x == 0) {
+        float *ds = diag_scratch + size_t(blockIdx.z) * NB * NB;
+        for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
+            uint32_t c = e / kb, r = e - c * kb;
+            ds[c * NB + r] = sF[c * LD + r];
+        }
+        return;
+    }
+    if (blockIdx.x <= nL) {
+        // row of L21: x U11 = a
+        uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
+        if (r >= m) return;
+        float a[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c) a[c] = (c < (int)kb) ? ld_cg(val + doff[k0 + c] + r) : 0.0f;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            if (c < (int)kb) {
+                float l = a[c] / sF[c * LD + c];
+                a[c] = l;
+#pragma unroll
+                for (int j = c + 1; j < NB; ++j) a[j] -= l * sF[j * LD + c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if (c < (int)kb) st_cg(val + doff[k0 + c] + r, a[c]);
+    } else {
+        // column of U12: L11 x = a
+        uint32_t j = r0 + (blockIdx.x - 1 - nL) * kPanelRows + tid;
+        if (j >= m) return;
+        const float *col = val + doff[j] + k0;
+        float a[NB];
+#pragma unroll
+        for (int r = 0; r < NB; ++r) a[r] = (r < (int)kb) ? ld_cg(col + r) : 0.0f;
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+            float u = a[r];
+#pragma unroll
+            for (int i = r + 1; i < NB; ++i) a[i] -= sF[r * LD + i] * u;
+        }
+        float *colw = val + doff[j] + k0;
+#pragma unroll
+        for (int r = 0; r < NB; ++r)
+            if (r < (int)kb) st_cg(colw + r, a[r]);
+    }
+}
+
+// Trailing update A22 -= L21 U12 on a 128 x 128 tile per block (256 threads,
+// 8 x 8 outputs each, K = kb <= 64 staged once in shared memory).  Block (0,0)
+// first writes the factored diagonal block back from diag_scratch.
+constexpr int kTB = kGemmTile;
+constexpr int kLDB = kTB + 4;
+constexpr int kLDC = kTB + 1;
+constexpr size_t kUpdateSmem =
+    (size_t(kDenseNB) * kTB + size_t(kDenseNB) * kLDB) * 4 > size_t(kTB) * kLDC * 4
+        ? (size_t(kDenseNB) * kTB + size_t(kDenseNB) * kLDB) * 4
+        : size_t(kTB) * kLDC * 4;
+
+__global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64_t stride,
+                                                         const uint32_t *__restrict__ doff,
+                                                         uint32_t m, uint32_t k0, uint32_t kb,
+                                                         const float *diag_scratch) {
+    extern __shared__ float4 smem4[];
+    float *smem = reinterpret_cast<float *>(smem4);
+    float *sA = smem;                       // [k][row]
+    float *sB = smem + kDenseNB * kTB;      // [k][col], padded
+    float *sC = smem;                       // [col][row], padded (reuses sA/sB)
+    float *val = val_base + blockIdx.z * stride;
+    const uint32_t tid = threadIdx.x;
+    if (blockIdx.x == 0 && blockIdx.y == 0) {
+        const float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
+        for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
+            uint32_t c = e / kb, r = e - c * kb;
+            st_cg(val + doff[k0 + c] + k0 + r, ds[c * kDenseNB + r]);
+        }
+    }
+    const uint32_t r0 = k0 + kb;
+    if (r0 >= m) return;
+    const uint32_t mp = m - r0;
+    const uint32_t rbase = blockIdx.x * kTB, cbase = blockIdx.y * kTB;
+    if (rbase >= mp || cbase >= mp) return;
+    const uint32_t tx = tid & 15, ty = tid >> 4;
+    // C tile into registers (through shared memory for coalescing): every
+    // entry then receives its updates one k at a time, in increasing k, as in
+    // the column algorithm.
+    for (uint32_t e = tid; e < uint32_t(kTB) * kTB; e += 256) {
+        uint32_t col = e / kTB, row = e - col * kTB;
+        float v = 0.0f;
+        if (cbase + col < mp && rbase + row < mp) v = ld_cg(val + doff[r0 + cbase + col] + r0 + rbase + row);
+        sC[col * kLDC + row] = v;
+    }
+    __syncthreads();
+    float acc[8][8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i][j] = sC[(tx * 8 + j) * kLDC + ty * 8 + i];
+    __syncthreads();
+    // stage L21 tile: sA[k][row]
+    for (uint32_t e = tid; e < uint32_t(kDenseNB) * kTB; e += 256) {
+        uint32_t k = e / kTB, row = e - k * kTB;
+        float v = 0.0f;
+        if (k < kb && rbase + row < mp) v = ld_cg(val + doff[k0 + k] + r0 + rbase + row);
+        sA[k * kTB + row] = v;
+    }
+    // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
+    {
+        uint32_t lane = tid & 31, w = tid >> 5;
+        for (uint32_t col = w; col < uint32_t(kTB); col += 8) {
+            bool cok = cbase + col < mp;
+            const float *src = cok ? val + doff[r0 + cbase + col] + k0 : nullptr;
+#pragma unroll
+            for (uint32_t h = 0; h < uint32_t(kDenseNB); h += 32) {
+                uint32_t k = h + lane;
+                float v = (cok && k < kb) ? ld_cg(src + k) : 0.0f;
+                sB[k * kLDB + col] = v;
+            }
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (uint32_t k = 0; k < kb; ++k) {
+        float4 a0 = *reinterpret_cast<const float4 *>(sA + k * kTB + ty * 8);
+        float4 a1 = *reinterpret_cast<const float4 *>(sA + k * kTB + ty * 8 + 4);
+        float4 b0 = *reinterpret_cast<const float4 *>(sB + k * kLDB + tx * 8);
+        float4 b1 = *reinterpret_cast<const float4 *>(sB + k * kLDB + tx * 8 + 4);
+        float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+        float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(-av[i], bv[j], acc[i][j]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) sC[(tx * 8 + j) * kLDC + ty * 8 + i] = acc[i][j];
+    __syncthreads();
+    for (uint32_t e = tid; e < uint32_t(kTB) * kTB; e += 256) {
+        uint32_t col = e / kTB, row = e - col * kTB;
+        if (cbase + col < mp && rbase + row < mp)
+            st_cg(val + doff[r0 + cbase + col] + r0 + rbase + row, sC[col * kLDC + row]);
+    }
+}
+
+cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
+                               uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
+                               float *diag_scratch, uint32_t last_has_l, cudaStream_t st) {
+    uint32_t rest = m - (k0 + kb);
+    uint32_t nL = (rest + kPanelRows - 1) / kPanelRows;
+    uint32_t nU = nL;
+    dim3 grid(1 + nL + nU, 1, count);
+    k_dense_panel<<<grid, kPanelRows, 0, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
+                                               last_has_l, nL);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
+                                uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
+                                cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_dense_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(kUpdateSmem));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    uint32_t rest = m - (k0 + kb);
+    uint32_t tiles = (rest + kTB - 1) / kTB;
+    if (tiles == 0) tiles = 1;
+    dim3 grid(tiles, tiles, count);
+    k_dense_update<<<grid, 256, kUpdateSmem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    return cudaGetLastError();
+}
+
+// --------------------------------------------------------------- utilities --
+__global__ void k_colsum(DevPattern P, const float *val_base, uint64_t stride, float *colmax) {
+    const float *val = val_base + blockIdx.z * stride;
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    float tmp = 0.0f;
+    if (c < P.n) {
+        // same order and precision as the reference's host loop (numeric.cu:495-502)
+        for (uint32_t p = P.cptr[c]; p < P.cptr[c + 1]; ++p) tmp += fabsf(val[p]);
+    }
+    // block max, then one atomic (non-negative floats compare as integers)
+    for (int o = 16; o > 0; o >>= 1) tmp = fmaxf(tmp, __shfl_xor_sync(0xffffffffu, tmp, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(colmax + blockIdx.z), __float_as_int(tmp));
+}
+
+__global__ void k_pert_finish(const float *colmax, float *pert_z, uint32_t count) {
+    uint32_t z = blockIdx.x * blockDim.x + threadIdx.x;
+    if (z < count) pert_z[z] = 3.45e-4f * colmax[z];
+}
+
+cudaError_t launch_pert(const DevPattern &P, const float *val, uint64_t stride, uint32_t count,
+                        float *colsum_scratch, float *pert_z, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(colsum_scratch, 0, sizeof(float) * count, st);
+    if (e != cudaSuccess) return e;
+    k_colsum<<<dim3((P.n + 255) / 256, 1, count), 256, 0, st>>>(P, val, stride, colsum_scratch);
+    k_pert_finish<<<(count + 255) / 256, 256, 0, st>>>(colsum_scratch, pert_z, count);
+    return cudaGetLastError();
+}
+
+__global__ void k_check_pivots(DevPattern P, const float *val_base, uint64_t stride, uint32_t *status) {
+    const float *val = val_base + blockIdx.z * stride;
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t flag = 0;
+    if (c < P.n) {
+        float d = val[P.diag[c]];
+        if (d == 0.0f) flag |= DEV_ZERO_PIVOT;
+        if (!isfinite(d)) flag |= DEV_NONFINITE_PIVOT;
+    }
+    flag = __reduce_or_sync(0xffffffffu, flag);
+    if (flag && (threadIdx.x & 31) == 0) atomicOr(status, flag);
+}
+
+cudaError_t launch_check_pivots(const DevPattern &P, const float *val, uint64_t stride,
+                                uint32_t count, uint32_t *status, cudaStream_t st) {
+    k_check_pivots<<<dim3((P.n + 255) / 256, 1, count), 256, 0, st>>>(P, val, stride, status);
+    return cudaGetLastError();
+}
+
+__global__ void k_gather_values(const int64_t *__restrict__ lu_src, const double *__restrict__ ax_base,
+                                uint64_t ax_stride, const double *__restrict__ scale, uint32_t nnz,
+                                float *val_base, uint64_t stride) {
+    const double *ax = ax_base + blockIdx.z * ax_stride;
+    float *val = val_base + blockIdx.z * stride;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += gridDim.x * blockDim.x) {
+        int64_t q = __ldg(lu_src + p);
+        float v = 0.0f;
+        if (q >= 0) {
+            double a = ax[q];
+            if (scale) a = a * __ldg(scale + q);
+            v = static_cast<float>(a);
+        }
+        val[p] = v;
+    }
+}
+
+cudaError_t launch_gather_values(const int64_t *lu_src, const double *ax, uint64_t ax_stride,
+                                 const double *scale, uint32_t nnz, float *val, uint64_t stride,
+                                 uint32_t count, cudaStream_t st) {
+    uint32_t blocks = (nnz + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks == 0) blocks = 1;
+    k_gather_values<<<dim3(blocks, 1, count), 256, 0, st>>>(lu_src, ax, ax_stride, scale, nnz, val, stride);
+    return cudaGetLastError();
+}
+
+}  // namespace glu

@@ -1,0 +1,130 @@
+// Kernel launchers of libglu_b200 (implemented in the .cu files).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "glu_common.cuh"
+
+namespace glu {
+
+// ------------------------------------------------------------ sparse factor --
+constexpr uint32_t kItemUnroll = 4;       // elements per lane per work item
+constexpr uint32_t kMaxItemBlocks = 148 * 16;
+constexpr uint32_t kChainThreads = 1024;
+
+// One level of the sparse schedule: its active columns are sched_cols[s0, s1),
+// processed by groups of G lanes, with atomics when atomic != 0.
+struct LevelInfo {
+    uint32_t s0, s1, G, atomic;
+};
+
+struct FactorPlanDev {
+    const uint32_t *sched_cols;  // active columns, level by level
+    const uint32_t *item_off;    // work-item prefix over sched_cols (per level G)
+    const LevelInfo *levels;     // per sparse level
+};
+
+cudaError_t launch_factor_level(const DevPattern &P, const FactorPlanDev &F, float *val,
+                                uint64_t stride, uint32_t count, const float *pert_z,
+                                const LevelInfo &cur, const LevelInfo *prev, uint32_t items,
+                                cudaStream_t st);
+cudaError_t launch_scale_level(const DevPattern &P, const FactorPlanDev &F, float *val,
+                               uint64_t stride, uint32_t count, const float *pert_z,
+                               const LevelInfo &lv, cudaStream_t st);
+// The cluster kernel itself (for occupancy queries).
+const void *chain_kernel_ptr();
+cudaError_t launch_factor_chain(const DevPattern &P, const FactorPlanDev &F, float *val,
+                                uint64_t stride, uint32_t count, const float *pert_z, uint32_t l0,
+                                uint32_t l1, uint32_t cluster, cudaStream_t st);
+
+// ------------------------------------------------------------- dense tail --
+// The trailing m x m block [t, n) x [t, n) is fully dense; element (i, j) of it
+// is val[doff[j] + i] (column-major, one base offset per column).
+constexpr int kDenseNB = 64;        // panel width
+constexpr int kPanelRows = 128;     // rows (or columns) per panel block
+constexpr int kGemmTile = 128;      // trailing-update tile
+
+cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
+                               uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
+                               float *diag_scratch, uint32_t last_has_l, cudaStream_t st);
+cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
+                                uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
+                                cudaStream_t st);
+
+// -------------------------------------------------------------- utilities --
+// pert[z] = 3.45e-4 * max_col sum |val| (FP32, column order), numeric.cu:490-506.
+cudaError_t launch_pert(const DevPattern &P, const float *val, uint64_t stride, uint32_t count,
+                        float *colsum_scratch, float *pert_z, cudaStream_t st);
+// ORs DEV_ZERO_PIVOT / DEV_NONFINITE_PIVOT into *status for bad pivots.
+cudaError_t launch_check_pivots(const DevPattern &P, const float *val, uint64_t stride,
+                                uint32_t count, uint32_t *status, cudaStream_t st);
+// LU values from source values: val[p] = src[p] < 0 ? 0 : (float)(ax[src[p]] * scale[src[p]]).
+cudaError_t launch_gather_values(const int64_t *lu_src, const double *ax, uint64_t ax_stride,
+                                 const double *scale, uint32_t nnz, float *val, uint64_t stride,
+                                 uint32_t count, cudaStream_t st);
+
+// ------------------------------------------------------------------ levels --
+// Level sets (symbolic.cc:106-151) built on the device; scratch must hold
+// level_scratch_bytes(n) bytes.
+size_t level_scratch_bytes(uint32_t n);
+cudaError_t build_levels(const DevPattern &P, void *scratch, int32_t *level_of, int32_t *level_ptr,
+                         int32_t *level_idx, int32_t *num_lev_dev, uint32_t *status,
+                         cudaStream_t st);
+
+// ------------------------------------------------------------------ solves --
+struct SolvePlanDev {
+    uint32_t t;                 // first column of the dense tail (n if none)
+    uint32_t m;                 // order of the dense tail
+    const uint32_t *doff;       // dense tail column offsets
+    const uint32_t *l_indeg;    // CSR entries left of the diagonal per row (L in-degree)
+    const uint32_t *u_indeg;    // CSR entries right of the diagonal per row (U in-degree)
+};
+
+// Transform in: y[j] = rhs[col_perm[piv[j]]] * (mc64 ? col_scale_perm[piv[j]] : 1)
+// (symbolic.cc:215-223); out: x[j] = y[row_perm_inv[j]] * (mc64 ? row_scale[j] : 1)
+// (symbolic.cc:242-247).  Transposed solves use the mirrored maps.
+struct TransformDev {
+    const uint32_t *in_idx;     // source index of each permuted entry
+    const double *in_scale;     // scale of each permuted entry (nullable)
+    const uint32_t *out_idx;
+    const double *out_scale;
+    const uint32_t *tin_idx;    // transposed: in
+    const double *tin_scale;
+    const uint32_t *tout_idx;   // transposed: out
+    const double *tout_scale;
+};
+
+// FP32 triangular solves on y (nrhs vectors of n, one after another), in place.
+cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
+                             float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
+                             uint32_t *status, cudaStream_t st);
+cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y,
+                        uint32_t nrhs, uint32_t *counters, uint32_t *ticket, uint32_t *status,
+                        cudaStream_t st);
+// Transposed: U^T z = y (forward), then L^T w = z (backward).
+cudaError_t solve_upper_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
+                              float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
+                              uint32_t *status, cudaStream_t st);
+cudaError_t solve_lower_unit_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
+                                   float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
+                                   uint32_t *status, cudaStream_t st);
+
+// Permute/scale kernels of the solve transforms.
+cudaError_t launch_transform_f32(const uint32_t *idx, const double *scale, const float *in,
+                                 float *out, uint32_t n, uint32_t nrhs, cudaStream_t st);
+cudaError_t launch_transform_f64_to_f32(const uint32_t *idx, const double *scale, const double *in,
+                                        float *out, uint32_t n, uint32_t nrhs, cudaStream_t st);
+cudaError_t launch_transform_f32_to_f64_add(const uint32_t *idx, const double *scale,
+                                            const float *in, double *x, uint32_t n, uint32_t nrhs,
+                                            int accumulate, cudaStream_t st);
+
+// FP64 residual r = b - A0 x (or A0^T) per right-hand side, with per-vector
+// sums of squares and max-abs accumulated into norms[2*v + {0,1}].
+cudaError_t launch_residual(const uint32_t *a_rptr, const uint32_t *a_cidx, const uint32_t *a_vmap,
+                            const double *ax0, uint32_t n, const double *b, const double *x,
+                            double *r, uint32_t nrhs, double *norms, cudaStream_t st);
+cudaError_t launch_norms(const double *v, uint32_t n, uint32_t nvec, double *norms,
+                         cudaStream_t st);
+
+}  // namespace glu

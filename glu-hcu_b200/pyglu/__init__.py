@@ -1,0 +1,441 @@
+"""pyglu -- Python interface of the B200 GLU sparse LU engine.
+
+Same surface as the reference's pyglu (pyglu/__init__.py, src/glu_binding.cpp):
+
+    lu = pyglu.splu(A)            # factorize (returns GLUFactorization)
+    x  = lu.solve(b)              # solve Ax = b
+    x  = pyglu.spsolve(A, b)      # factorize and solve in one call
+
+A is any scipy sparse matrix or a (data, indices, indptr, shape) CSC tuple.
+As in the reference, the factors and the plain solve are FP32 (inputs and
+outputs are float64, converted at the boundary); unlike the reference the
+solve runs on the GPU.  Additions:
+
+* ``lu.solve(b, refine=True, tol=1e-10)`` -- FP64 iterative refinement on the
+  GPU (residuals with the original FP64 matrix), reaching FP64-level residuals;
+* ``lu.refactor(data)`` -- new values, same pattern, no new analysis;
+* ``lu.solve(b, trans='T')`` -- solves with A^T;
+* :class:`BatchedGLU` -- many value sets of one pattern factored and solved
+  together;
+* :func:`sparse_solve` -- differentiable solve (torch.autograd.Function) with
+  a hand-written adjoint;
+* :func:`tune` -- the schedule autotuner.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+try:
+    import scipy.sparse as _sp
+
+    _HAS_SCIPY = True
+except ImportError:  # pragma: no cover
+    _HAS_SCIPY = False
+
+from . import _capi
+from ._capi import GLUError, NotConvergedError, SingularMatrixError, check, ptr
+
+__all__ = ["splu", "spsolve", "GLUFactorization", "BatchedGLU", "sparse_solve", "tune",
+           "GLUError", "SingularMatrixError", "NotConvergedError", "read_mtx"]
+
+
+def _to_csc_arrays(A):
+    """Return (data_f64, indices_i32, indptr_i32, n) from a sparse matrix.
+
+    Same validation and messages as the reference (pyglu/__init__.py:30-63).
+    """
+    if _HAS_SCIPY and _sp.issparse(A):
+        A = A.tocsc()
+        A.sum_duplicates()
+        A.sort_indices()
+        n = A.shape[0]
+        if A.shape[0] != A.shape[1]:
+            raise ValueError(f"Matrix must be square, got shape {A.shape}")
+        data = np.ascontiguousarray(A.data, dtype=np.float64)
+        indices = np.ascontiguousarray(A.indices, dtype=np.int32)
+        indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    elif isinstance(A, tuple) and len(A) == 4:
+        data, indices, indptr, shape = A
+        n = shape[0]
+        if shape[0] != shape[1]:
+            raise ValueError(f"Matrix must be square, got shape {shape}")
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        indices = np.ascontiguousarray(indices, dtype=np.int32)
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+    else:
+        raise TypeError(
+            "A must be a scipy sparse matrix or a "
+            "(data, indices, indptr, shape) tuple in CSC format"
+        )
+    if len(indptr) != n + 1:
+        raise ValueError(f"indptr length {len(indptr)} inconsistent with n={n}")
+    if n == 0:
+        raise ValueError("Matrix dimension must be > 0")
+    return data, indices, indptr, n
+
+
+def _validate(data, indices, indptr, n):
+    """Checks of the reference binding (src/glu_binding.cpp:51-77)."""
+    if n <= 0:
+        raise ValueError("n must be positive")
+    data = np.ascontiguousarray(data, dtype=np.float64)
+    indices = np.ascontiguousarray(indices, dtype=np.int32)
+    indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+    if indices.shape[0] != data.shape[0]:
+        raise ValueError("data and indices length mismatch")
+    if indptr.shape[0] != n + 1:
+        raise ValueError("indptr length must be n+1")
+    if (indices < 0).any():
+        raise ValueError("Negative row index in CSC matrix")
+    if (indptr < 0).any():
+        raise ValueError("Negative indptr value")
+    return data, indices.astype(np.uint32), indptr.astype(np.uint32)
+
+
+class Analysis:
+    """NICSLU preprocessing plus the symbolic phase of one sparsity pattern.
+
+    Holds the preprocessed matrix, the permutations/scalings used by the
+    solves, the map from the input matrix's entries into the LU layout, and
+    the L+U pattern (the reference's Symbolic_Matrix arrays).
+    """
+
+    def __init__(self, data, indices, indptr, n):
+        data, ai, ap = _validate(data, indices, indptr, n)
+        if data.size == 0:
+            raise RuntimeError("GLU preprocessing failed (error -1)")
+        pre = _capi.pre()
+        h = _capi.C.c_void_p()
+        ret = pre.glu_pre_analyze(n, data.size, ptr(data), ptr(ai), ptr(ap), _capi.C.byref(h))
+        if ret != 0:
+            raise RuntimeError(f"GLU preprocessing failed (error {ret})")
+        try:
+            nz = pre.glu_pre_nnz(h)
+            self.n = n
+            self.nnz_a = nz
+            self.pax = np.empty(nz, np.float64)
+            self.pai = np.empty(nz, np.uint32)
+            self.pap = np.empty(n + 1, np.uint32)
+            pre.glu_pre_matrix(h, ptr(self.pax), ptr(self.pai), ptr(self.pap))
+            self.col_perm = np.empty(n, np.uint32)
+            self.row_perm_inv = np.empty(n, np.uint32)
+            self.pivot = np.empty(n, np.int32)
+            self.col_scale_perm = np.empty(n, np.float64)
+            self.row_scale = np.empty(n, np.float64)
+            mc = _capi.C.c_int(0)
+            pre.glu_pre_transform(h, ptr(self.col_perm), ptr(self.row_perm_inv), ptr(self.pivot),
+                                  ptr(self.col_scale_perm), ptr(self.row_scale), _capi.C.byref(mc))
+            self.mc64 = int(mc.value)
+            self.src_pos = np.empty(nz, np.uint32)
+            self.src_scale = np.empty(nz, np.float64)
+            pre.glu_pre_source_map(h, ptr(self.src_pos), ptr(self.src_scale))
+        finally:
+            pre.glu_pre_destroy(h)
+        self.data, self.ai, self.ap = data, ai, ap
+        eng = _capi.engine()
+        self._sym = _capi.C.c_void_p()
+        check(eng.glu_symbolic_analyze(n, nz, ptr(self.pap), ptr(self.pai), _capi.C.byref(self._sym)),
+              "symbolic analysis")
+        nlu = _capi.C.c_uint32(0)
+        eng.glu_symbolic_sizes(self._sym, None, _capi.C.byref(nlu))
+        self.nnz_lu = int(nlu.value)
+        slots = np.empty(nz, np.uint32)
+        eng.glu_symbolic_slots(self._sym, ptr(slots))
+        self.slots = slots
+        self.src_slot = np.ascontiguousarray(slots[self.src_pos])
+
+    def pattern(self):
+        """The L+U pattern: dict of the Symbolic_Matrix arrays (include/symbolic.h:15-21)."""
+        n, z = self.n, self.nnz_lu
+        out = dict(sym_c_ptr=np.empty(n + 1, np.uint32), sym_r_idx=np.empty(z, np.uint32),
+                   l_col_ptr=np.empty(n, np.uint32), csr_r_ptr=np.empty(n + 1, np.uint32),
+                   csr_c_idx=np.empty(z, np.uint32), csr_diag_ptr=np.empty(n, np.uint32))
+        _capi.engine().glu_symbolic_export(self._sym, *(ptr(out[k]) for k in (
+            "sym_c_ptr", "sym_r_idx", "l_col_ptr", "csr_r_ptr", "csr_c_idx", "csr_diag_ptr")))
+        return out
+
+    def predict_lu(self, pax=None):
+        """predictLU (src/symbolic.cc:82-103): FP32 LU values from the preprocessed FP64 values."""
+        pax = self.pax if pax is None else np.ascontiguousarray(pax, np.float64)
+        val = np.empty(self.nnz_lu, np.float32)
+        _capi.engine().glu_predict_lu(self._sym, ptr(pax), ptr(val))
+        return val
+
+    def __del__(self):
+        try:
+            _capi.engine().glu_symbolic_destroy(self._sym)
+        except Exception:
+            pass
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _stream():
+    torch = _torch()
+    return _capi.C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class _Engine:
+    """A device handle for `batch` value sets of one analysed pattern."""
+
+    def __init__(self, an: Analysis, batch=1, device=0):
+        eng = _capi.engine()
+        self.an = an
+        self.batch = batch
+        self.device = device
+        self._h = _capi.C.c_void_p()
+        check(eng.glu_create(an._sym, device, batch, _capi.C.byref(self._h)), "device setup")
+        check(eng.glu_set_transform(self._h, ptr(an.col_perm), ptr(an.row_perm_inv), ptr(an.pivot),
+                                    ptr(an.col_scale_perm), ptr(an.row_scale), an.mc64), "transform setup")
+        check(eng.glu_set_source(self._h, an.nnz_a, ptr(an.ap), ptr(an.ai), ptr(an.src_slot),
+                                 ptr(an.src_scale)), "source setup")
+
+    def __del__(self):
+        try:
+            _capi.engine().glu_destroy(self._h)
+        except Exception:
+            pass
+
+
+def _is_cuda_tensor(x):
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+class GLUFactorization:
+    """GPU LU factorization of a sparse matrix (same constructor as the reference).
+
+    Constructed by :func:`splu`.  Call ``.solve(b)`` to solve ``Ax = b``.
+    """
+
+    def __init__(self, data, indices, indptr, n, perturb=False, device=0):
+        self._an = Analysis(data, indices, indptr, n)
+        self._eng = _Engine(self._an, 1, device)
+        self.perturb = bool(perturb)
+        self._factor_values(self._an.data)
+
+    # -- reference surface -------------------------------------------------
+    @property
+    def n(self):
+        """Matrix dimension."""
+        return self._an.n
+
+    def solve(self, b, refine=False, tol=1e-10, maxiter=10, trans="N"):
+        """Solve ``A x = b`` (``trans='T'``: ``A^T x = b``).
+
+        b has shape (n,) or (n, k).  Without ``refine`` this is the reference's
+        FP32 solve (b cast to float32, result returned as float64); with it,
+        FP64 iterative refinement to relative residual ``tol``.
+        """
+        b = np.asarray(b, dtype=np.float64)
+        n = self.n
+        if b.shape[0] != n:
+            raise ValueError(f"RHS length {b.shape[0]} != matrix dimension {n}")
+        vec = b.ndim == 1
+        bm = np.ascontiguousarray(b.reshape(n, -1).T)  # (k, n)
+        k = bm.shape[0]
+        t = 1 if str(trans).upper() in ("T", "H") else 0
+        eng = _capi.engine()
+        if refine:
+            x = np.empty_like(bm)
+            st = _capi.RefineStats()
+            s = eng.glu_solve_refined(self._eng._h, 0, 1, k, ptr(bm), ptr(x), float(tol), int(maxiter), t,
+                                      _capi.GLU_HOST, _capi.C.byref(st), None)
+            self.last_refine = dict(iterations=st.iterations, residual=st.residual,
+                                    residual_inf=st.residual_inf)
+            if s != _capi.GLU_ERR_NOT_CONVERGED:
+                check(s, "refined solve")
+        else:
+            bf = bm.astype(np.float32)
+            xf = np.empty_like(bf)
+            fn = eng.glu_solve_transposed if t else eng.glu_solve
+            check(fn(self._eng._h, 0, k, ptr(bf), ptr(xf), _capi.GLU_HOST, None), "solve")
+            x = xf.astype(np.float64)
+        x = x.T
+        return np.ascontiguousarray(x[:, 0] if vec else x)
+
+    # -- additions ---------------------------------------------------------
+    def _factor_values(self, data):
+        eng = _capi.engine()
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        if data.shape != (self._an.nnz_a,):
+            raise ValueError(f"expected {self._an.nnz_a} values, got shape {data.shape}")
+        check(eng.glu_load_source_values(self._eng._h, 0, 1, ptr(data), _capi.GLU_HOST, None), "value upload")
+        check(eng.glu_factor(self._eng._h, 0, 1, 1 if self.perturb else 0, None), "GPU factorization")
+
+    def refactor(self, data):
+        """Refactorize with new values of the same pattern (the data array of
+        the CSC matrix in the same order as the one given to the constructor)."""
+        self._factor_values(data)
+        return self
+
+    def refactor_device(self, data, stream=None):
+        """Refactorize from a CUDA float64 tensor of values (no host round trip)."""
+        eng = _capi.engine()
+        st = stream if stream is not None else _stream()
+        check(eng.glu_load_source_values(self._eng._h, 0, 1, _capi.C.c_void_p(data.data_ptr()),
+                                         _capi.GLU_DEVICE, st), "value upload")
+        check(eng.glu_factor(self._eng._h, 0, 1, 1 if self.perturb else 0, st), "GPU factorization")
+
+    def solve_device(self, b, x, refine=True, tol=1e-10, maxiter=10, trans="N", stream=None):
+        """Solve with CUDA float64 tensors b, x of shape (k, n) (refined) or
+        float32 (plain); returns the refinement statistics."""
+        eng = _capi.engine()
+        st = stream if stream is not None else _stream()
+        k = b.shape[0] if b.dim() == 2 else 1
+        t = 1 if str(trans).upper() in ("T", "H") else 0
+        bp = _capi.C.c_void_p(b.data_ptr())
+        xp = _capi.C.c_void_p(x.data_ptr())
+        if refine:
+            rs = _capi.RefineStats()
+            s = eng.glu_solve_refined(self._eng._h, 0, 1, k, bp, xp, float(tol), int(maxiter), t,
+                                      _capi.GLU_DEVICE, _capi.C.byref(rs), st)
+            if s != _capi.GLU_ERR_NOT_CONVERGED:
+                check(s, "refined solve")
+            return dict(iterations=rs.iterations, residual=rs.residual, residual_inf=rs.residual_inf)
+        fn = eng.glu_solve_transposed if t else eng.glu_solve
+        check(fn(self._eng._h, 0, k, bp, xp, _capi.GLU_DEVICE, st), "solve")
+        return None
+
+    def lu_values(self):
+        """FP32 factor values in the Symbolic_Matrix::val layout."""
+        val = np.empty(self._an.nnz_lu, np.float32)
+        check(_capi.engine().glu_store_lu_values(self._eng._h, 0, 1, ptr(val), _capi.GLU_HOST, None), "read values")
+        return val
+
+    def pattern(self):
+        return self._an.pattern()
+
+    def levels(self):
+        """(level_ptr, level_idx) built on the GPU."""
+        eng = _capi.engine()
+        nl = _capi.C.c_int32(0)
+        eng.glu_levels(self._eng._h, _capi.C.byref(nl), None, None)
+        lp = np.empty(nl.value + 1, np.int32)
+        li = np.empty(self.n, np.int32)
+        eng.glu_levels(self._eng._h, None, ptr(lp), ptr(li))
+        return lp, li
+
+    @property
+    def stats(self):
+        st = _capi.Stats()
+        _capi.engine().glu_get_stats(self._eng._h, _capi.C.byref(st))
+        return {k: getattr(st, k) for k, _ in _capi.Stats._fields_}
+
+    @property
+    def analysis(self):
+        return self._an
+
+    @property
+    def handle(self):
+        return self._eng._h
+
+
+def splu(A, perturb=False, device=0):
+    """Compute the sparse LU factorization of A on the GPU.
+
+    Parameters
+    ----------
+    A : scipy.sparse matrix (any format) or (data, indices, indptr, shape) tuple
+    perturb : bool, optional -- GESP diagonal perturbation for tiny pivots.
+
+    Raises ValueError for a non-square or inconsistent matrix, RuntimeError when
+    preprocessing or the GPU factorization fails.
+    """
+    data, indices, indptr, n = _to_csc_arrays(A)
+    return GLUFactorization(data, indices, indptr, n, perturb, device)
+
+
+def spsolve(A, b, perturb=False, refine=False, tol=1e-10):
+    """Solve the sparse linear system Ax = b on the GPU."""
+    b = np.asarray(b, dtype=np.float64)
+    return splu(A, perturb=perturb).solve(b, refine=refine, tol=tol)
+
+
+class BatchedGLU:
+    """Many value sets of one sparsity pattern, factored and solved together.
+
+    ``values`` has shape (B, nnz) in the data order of the CSC pattern
+    (data, indices, indptr).  NICSLU's ordering and scaling are computed once
+    from ``values[0]`` and reused for every set, as NICSLU's own refactor does
+    (NicsLU_ResetMatrixValues, nicslu_matrix.c:244-269).
+    """
+
+    def __init__(self, indices, indptr, n, values, perturb=False, device=0):
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        if values.ndim != 2:
+            raise ValueError("values must have shape (B, nnz)")
+        self._an = Analysis(values[0], indices, indptr, n)
+        self.batch = values.shape[0]
+        self._eng = _Engine(self._an, self.batch, device)
+        self.perturb = bool(perturb)
+        self.refactor(values)
+
+    @property
+    def n(self):
+        return self._an.n
+
+    def refactor(self, values):
+        eng = _capi.engine()
+        values = np.ascontiguousarray(values, dtype=np.float64)
+        if values.shape != (self.batch, self._an.nnz_a):
+            raise ValueError(f"values must have shape ({self.batch}, {self._an.nnz_a})")
+        check(eng.glu_load_source_values(self._eng._h, 0, self.batch, ptr(values), _capi.GLU_HOST, None),
+              "value upload")
+        status = eng.glu_factor(self._eng._h, 0, self.batch, 1 if self.perturb else 0, None)
+        check(status, "GPU factorization")
+
+    def solve(self, b, tol=1e-10, maxiter=10, refine=True):
+        """b: (B, k, n) float64 -> x (B, k, n), FP64-refined."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        if b.ndim == 2:
+            b = b[:, None, :]
+        B, k, n = b.shape
+        if B != self.batch or n != self.n:
+            raise ValueError("b must have shape (B, k, n)")
+        x = np.empty_like(b)
+        st = _capi.RefineStats()
+        s = _capi.engine().glu_solve_refined(self._eng._h, 0, B, k, ptr(b), ptr(x), float(tol), int(maxiter),
+                                             0, _capi.GLU_HOST, _capi.C.byref(st), None)
+        self.last_refine = dict(iterations=st.iterations, residual=st.residual, residual_inf=st.residual_inf)
+        if s != _capi.GLU_ERR_NOT_CONVERGED:
+            check(s, "refined solve")
+        return x
+
+    @property
+    def handle(self):
+        return self._eng._h
+
+    @property
+    def stats(self):
+        st = _capi.Stats()
+        _capi.engine().glu_get_stats(self._eng._h, _capi.C.byref(st))
+        return {k: getattr(st, k) for k, _ in _capi.Stats._fields_}
+
+
+def read_mtx(path):
+    """Matrix Market file -> (data, indices, indptr, n) with NICSLU's reader."""
+    import ctypes as C
+
+    pre = _capi.pre()
+    n = C.c_uint32(0)
+    nz = C.c_uint32(0)
+    ax, ai, ap = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    ret = pre.glu_pre_read_mtx(str(path).encode(), C.byref(n), C.byref(nz), C.byref(ax), C.byref(ai), C.byref(ap))
+    if ret != 0:
+        raise RuntimeError(f"cannot read {path} (NICSLU error {ret})")
+    try:
+        data = np.ctypeslib.as_array(C.cast(ax, C.POINTER(C.c_double)), (nz.value,)).copy()
+        indices = np.ctypeslib.as_array(C.cast(ai, C.POINTER(C.c_uint32)), (nz.value,)).astype(np.int32)
+        indptr = np.ctypeslib.as_array(C.cast(ap, C.POINTER(C.c_uint32)), (n.value + 1,)).astype(np.int32)
+    finally:
+        for p in (ax, ai, ap):
+            pre.glu_pre_free(p)
+    return data, indices, indptr, int(n.value)
+
+
+from .autograd import sparse_solve  # noqa: E402
+from .autotune import tune  # noqa: E402
