@@ -100,8 +100,9 @@ struct glu_handle_s {
     // factor plan
     glu_tuning tune{};
     uint32_t t = 0, m = 0;
-    std::vector<uint32_t> doff_h;
-    DevBuf d_doff, d_sched, d_item_off, d_levels;
+    bool dense_buffer = false;  // tail factored in d_dense (not in place)
+    std::vector<uint32_t> doff_h, tail_start_h;
+    DevBuf d_doff, d_tail_start, d_dense, d_sched, d_item_off, d_levels;
     std::vector<LevelInfo> levels_h;
     std::vector<uint32_t> items_h;
     std::vector<uint64_t> work_h;
@@ -110,7 +111,8 @@ struct glu_handle_s {
     FactorPlanDev F{};
     double flops = 0;
     // solve plan
-    DevBuf d_lneed, d_uneed;
+    DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
+    std::vector<SweepStep> sw_steps[4];
     SolvePlanDev S{};
     // transforms (forward in/out, transposed in/out)
     DevBuf d_tr[8];
@@ -157,7 +159,7 @@ struct DeviceGuard {
 inline cudaStream_t S_(glu_stream s) { return static_cast<cudaStream_t>(s); }
 
 // Largest trailing block [t, n) in which every entry is in the pattern.
-void find_dense_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t &m) {
+void find_full_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t &m) {
     const uint32_t n = s.n;
     // run[j]: first row of the contiguous run of rows ending at n-1 in column j
     std::vector<uint32_t> run(n);
@@ -187,6 +189,128 @@ void find_dense_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_
     }
 }
 
+// Cost model of the split point t: the columns [t, n) are factored as a dense
+// block, the columns in front of t level by level.  Dense: 2/3 m^3 flops at
+// kDenseRate plus kPanelLatency per panel step.  Sparse: the update work of
+// the columns < t at kSparseRate plus kLevelLatency per level that still has
+// an active column < t.  Returns the t of least estimated time with
+// m <= max_m (t = n: no dense tail).
+constexpr double kDenseRate = 30e12, kPanelLatency = 20e-6;
+constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
+
+uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
+                      const std::vector<int32_t> &level_idx, uint32_t max_m) {
+    const uint32_t n = s.n;
+    // sparse work of column k and the first column of each level
+    std::vector<double> pre(n + 1, 0.0);
+    for (uint32_t k = 0; k < n; ++k) {
+        double L = s.sym_c_ptr[k + 1] - s.l_col_ptr[k] - 1;
+        double U = s.csr_r_ptr[k + 1] - s.csr_diag_ptr[k] - 1;
+        pre[k + 1] = pre[k] + L + 2 * L * U;
+    }
+    std::vector<uint32_t> lev_first;
+    for (size_t l = 0; l + 1 < level_ptr.size(); ++l) {
+        uint32_t first = n;
+        for (int32_t q = level_ptr[l]; q < level_ptr[l + 1]; ++q) {
+            uint32_t k = uint32_t(level_idx[q]);
+            if (s.l_col_ptr[k] + 1 != s.sym_c_ptr[k + 1]) {
+                first = k;  // ascending within a level
+                break;
+            }
+        }
+        if (first < n) lev_first.push_back(first);
+    }
+    std::sort(lev_first.begin(), lev_first.end());
+    double best = 1e300;
+    uint32_t best_t = n;
+    const int64_t lo = max_m >= n ? 0 : int64_t(n) - max_m;
+    for (int64_t tt = n; tt >= lo; tt -= 16) {
+        const uint32_t t = uint32_t(tt);
+        double m = double(n - t);
+        double dense = m > 0 ? (2.0 / 3.0) * m * m * m / kDenseRate + std::ceil(m / kDenseNB) * kPanelLatency : 0;
+        double nlev = double(std::lower_bound(lev_first.begin(), lev_first.end(), t) - lev_first.begin());
+        double sparse = pre[t] / kSparseRate + nlev * kLevelLatency;
+        if (dense + sparse < best) {
+            best = dense + sparse;
+            best_t = t;
+        }
+    }
+    return best_t;
+}
+
+// Level schedule of one sparse sweep over the columns [0, t) (tail columns are
+// solved before or after it densely).  Dependencies:
+//   L  (forward, scatter):  j needs c < j with L(j,c) != 0  (CSR row j left of diag)
+//   U  (backward, scatter): j needs c > j with U(j,c) != 0  (CSR row j right of diag)
+//   U^T (forward, gather):  j needs i < j with U(i,j) != 0  (CSC column j above diag)
+//   L^T (backward, gather): j needs i > j with L(i,j) != 0  (CSC column j below diag)
+// Work items of pivot j: its entries in chunks of kSweepChunk (at least one,
+// the dividing sweeps store x_j).  Levels with more than `thin` items get
+// their own launch; runs of thinner levels go to the cluster kernel.
+void build_sweep(const SymbolicData &s, uint32_t t, int mode, uint32_t thin, std::vector<uint32_t> &cols,
+                 std::vector<uint32_t> &lptr, std::vector<uint32_t> &item_off, std::vector<SweepStep> &steps) {
+    std::vector<int32_t> lev(t, 0);
+    int32_t nlev = 0;
+    const bool forward = (mode == SWEEP_L || mode == SWEEP_UT);
+    for (uint32_t q = 0; q < t; ++q) {
+        const uint32_t j = forward ? q : t - 1 - q;
+        int32_t mx = -1;
+        if (mode == SWEEP_L) {
+            for (uint32_t e = s.csr_r_ptr[j]; e < s.csr_diag_ptr[j]; ++e) mx = std::max(mx, lev[s.csr_c_idx[e]]);
+        } else if (mode == SWEEP_U) {
+            for (uint32_t e = s.csr_diag_ptr[j] + 1; e < s.csr_r_ptr[j + 1]; ++e) {
+                uint32_t c = s.csr_c_idx[e];
+                if (c < t) mx = std::max(mx, lev[c]);
+            }
+        } else if (mode == SWEEP_UT) {
+            for (uint32_t p = s.sym_c_ptr[j]; p < s.l_col_ptr[j]; ++p) mx = std::max(mx, lev[s.sym_r_idx[p]]);
+        } else {
+            for (uint32_t p = s.l_col_ptr[j] + 1; p < s.sym_c_ptr[j + 1]; ++p) {
+                uint32_t i = s.sym_r_idx[p];
+                if (i < t) mx = std::max(mx, lev[i]);
+            }
+        }
+        lev[j] = mx + 1;
+        nlev = std::max(nlev, mx + 2);
+    }
+    lptr.assign(size_t(nlev) + 1, 0);
+    for (uint32_t j = 0; j < t; ++j) lptr[lev[j] + 1]++;
+    for (int32_t l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
+    cols.assign(t, 0);
+    {
+        std::vector<uint32_t> cur(lptr.begin(), lptr.end() - 1);
+        for (uint32_t j = 0; j < t; ++j) cols[cur[lev[j]]++] = j;
+    }
+    item_off.assign(size_t(t) + 1, 0);
+    for (uint32_t q = 0; q < t; ++q) {
+        const uint32_t j = cols[q];
+        uint32_t len;
+        if (mode == SWEEP_L)
+            len = s.sym_c_ptr[j + 1] - s.l_col_ptr[j] - 1;
+        else if (mode == SWEEP_U)
+            len = s.l_col_ptr[j] - s.sym_c_ptr[j];
+        else if (mode == SWEEP_UT)
+            len = s.csr_r_ptr[j + 1] - s.csr_diag_ptr[j] - 1;
+        else
+            len = s.csr_diag_ptr[j] - s.csr_r_ptr[j];
+        item_off[q + 1] = item_off[q] + std::max<uint32_t>(1, (len + kSweepChunk - 1) / kSweepChunk);
+    }
+    auto items = [&](int32_t l) { return item_off[lptr[l + 1]] - item_off[lptr[l]]; };
+    steps.clear();
+    int32_t l = 0;
+    while (l < nlev) {
+        if (items(l) > thin) {
+            steps.push_back(SweepStep{0, uint32_t(l), uint32_t(l + 1), lptr[l], lptr[l + 1]});
+            ++l;
+        } else {
+            int32_t e = l;
+            while (e < nlev && items(e) <= thin) ++e;
+            steps.push_back(SweepStep{1, uint32_t(l), uint32_t(e), lptr[l], lptr[e]});
+            l = e;
+        }
+    }
+}
+
 uint32_t pick_group(double avg_l, uint32_t forced) {
     if (forced) return forced;
     if (avg_l <= 6) return 4;
@@ -198,10 +322,48 @@ uint32_t pick_group(double avg_l, uint32_t forced) {
 Status build_plan(glu_handle_s *h) {
     const SymbolicData &s = h->pat;
     const uint32_t n = h->n;
-    find_dense_tail(s, h->tune.dense_tail_min, h->t, h->m);
+    // split point: fully dense trailing block (factored in place) or, when the
+    // cost model prefers a larger block, a dense buffer of order <= max_m
+    uint32_t t_full, m_full;
+    find_full_tail(s, 1, t_full, m_full);
+    uint32_t max_m = h->tune.dense_tail_max;
+    {
+        // buffers for every value set must fit in a fraction of free memory
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b > 0) {
+            double cap = std::sqrt(0.4 * double(free_b) / (4.0 * h->batch));
+            if (cap < max_m) max_m = uint32_t(cap);
+        }
+    }
+    uint32_t t_opt = choose_split(s, h->level_ptr, h->level_idx, std::max(max_m, m_full));
+    h->dense_buffer = false;
+    if (t_opt >= t_full) {
+        h->t = t_opt;  // any trailing block of a fully dense block is fully dense
+    } else if (n - t_opt <= max_m) {
+        h->t = t_opt;
+        h->dense_buffer = true;
+    } else {
+        h->t = t_full;
+    }
+    h->m = n - h->t;
+    if (h->m < h->tune.dense_tail_min) {
+        h->t = n;
+        h->m = 0;
+        h->dense_buffer = false;
+    }
     const uint32_t t = h->t, m = h->m;
     h->doff_h.assign(std::max<uint32_t>(m, 1), 0);
-    for (uint32_t j = 0; j < m; ++j) h->doff_h[j] = s.sym_c_ptr[t + j + 1] - m;
+    h->tail_start_h.assign(std::max<uint32_t>(m, 1), 0);
+    for (uint32_t j = 0; j < m; ++j) {
+        const uint32_t *b0 = s.sym_r_idx.data() + s.sym_c_ptr[t + j];
+        const uint32_t *b1 = s.sym_r_idx.data() + s.sym_c_ptr[t + j + 1];
+        h->tail_start_h[j] = uint32_t(std::lower_bound(b0, b1, t) - s.sym_r_idx.data());
+        h->doff_h[j] = h->dense_buffer ? j * m : h->tail_start_h[j];
+    }
+    h->d_dense.release();
+    if (h->dense_buffer)
+        GLU_CUDA(h->d_dense.alloc(sizeof(float) * size_t(m) * m * h->batch), "allocate dense tail buffer");
+    GLU_CUDA(upload(h->d_tail_start, h->tail_start_h), "upload dense offsets");
 
     std::vector<uint32_t> sched, item_off(1, 0);
     h->levels_h.clear();
@@ -275,20 +437,37 @@ Status build_plan(glu_handle_s *h) {
     h->F.item_off = h->d_item_off.as<uint32_t>();
     h->F.levels = h->d_levels.as<LevelInfo>();
 
-    // solve plan: dependency counts of the sparse sweeps
-    std::vector<uint32_t> lneed(n, 0), uneed(n, 0);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (uint32_t e = s.csr_r_ptr[i]; e < s.csr_diag_ptr[i]; ++e)
-            if (s.csr_c_idx[e] < t) ++lneed[i];
-        uneed[i] = s.csr_r_ptr[i + 1] - s.csr_diag_ptr[i] - 1;
-    }
-    GLU_CUDA(upload(h->d_lneed, lneed), "upload solve plan");
-    GLU_CUDA(upload(h->d_uneed, uneed), "upload solve plan");
+    // solve plan: level schedules of the four sparse sweeps
     h->S.t = t;
     h->S.m = m;
     h->S.doff = h->d_doff.as<uint32_t>();
-    h->S.l_indeg = h->d_lneed.as<uint32_t>();
-    h->S.u_indeg = h->d_uneed.as<uint32_t>();
+    h->S.tail_start = h->d_tail_start.as<uint32_t>();
+    h->S.cluster = h->tune.solve_cluster ? h->tune.solve_cluster : 4;
+    {
+        // CSR position of the first column >= t in every tail row
+        std::vector<uint32_t> trs(std::max<uint32_t>(m, 1), 0);
+        for (uint32_t i = 0; i < m; ++i) {
+            const uint32_t *b0 = s.csr_c_idx.data() + s.csr_r_ptr[t + i];
+            const uint32_t *b1 = s.csr_c_idx.data() + s.csr_r_ptr[t + i + 1];
+            trs[i] = uint32_t(std::lower_bound(b0, b1, t) - s.csr_c_idx.data());
+        }
+        GLU_CUDA(upload(h->d_tail_row_start, trs), "upload solve plan");
+        h->S.tail_row_start = h->d_tail_row_start.as<uint32_t>();
+    }
+    for (int mode = 0; mode < 4; ++mode) {
+        std::vector<uint32_t> cols, lptr, ioff;
+        build_sweep(s, t, mode, h->tune.solve_thin, cols, lptr, ioff, h->sw_steps[mode]);
+        GLU_CUDA(upload(h->d_sw_cols[mode], cols), "upload solve plan");
+        GLU_CUDA(upload(h->d_sw_lptr[mode], lptr), "upload solve plan");
+        GLU_CUDA(upload(h->d_sw_ioff[mode], ioff), "upload solve plan");
+        SweepPlan &sp = h->S.sweep[mode];
+        sp.cols = h->d_sw_cols[mode].as<uint32_t>();
+        sp.lptr = h->d_sw_lptr[mode].as<uint32_t>();
+        sp.item_off = h->d_sw_ioff[mode].as<uint32_t>();
+        sp.steps = h->sw_steps[mode].data();
+        sp.nsteps = uint32_t(h->sw_steps[mode].size());
+        sp.nlev = uint32_t(lptr.size() - 1);
+    }
 
     uint32_t wide = 0, chains = 0;
     for (auto &st : h->steps) (st.kind == STEP_CHAIN ? chains : wide)++;
@@ -329,7 +508,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 1.0f};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 16384u, 128u, 4u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -421,17 +600,22 @@ Status read_status(glu_handle_s *h, cudaStream_t st, uint32_t *flags) {
     return GLU_OK;
 }
 
-// One FP32 solve of y in place (nrhs vectors of n), in the permuted system.
-Status solve_inplace(glu_handle_s *h, const float *val, float *y, uint32_t nrhs, bool trans, cudaStream_t st) {
+// One FP32 solve of y in place (nrhs vectors of n), in the permuted system,
+// with the factors of value set z.
+Status solve_inplace(glu_handle_s *h, uint32_t z, float *y, uint32_t nrhs, bool trans, cudaStream_t st) {
     uint32_t *cnt = h->d_counters.as<uint32_t>();
     uint32_t *tk = h->d_ticket.as<uint32_t>();
     uint32_t *status = h->d_status.as<uint32_t>();
+    const float *val = h->d_val.as<float>() + size_t(z) * h->nnz;
+    const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(z) * h->m * h->m : val;
+    GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs), "allocate solve buffer");
+    float *xo = h->d_xo.as<float>();
     if (!trans) {
-        GLU_CUDA(solve_lower_unit(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "lower solve");
-        GLU_CUDA(solve_upper(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "upper solve");
+        GLU_CUDA(solve_lower_unit(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "lower solve");
+        GLU_CUDA(solve_upper(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "upper solve");
     } else {
-        GLU_CUDA(solve_upper_trans(h->P, h->S, val, y, nrhs, cnt, tk, status, st), "transposed upper solve");
-        GLU_CUDA(solve_lower_unit_trans(h->P, h->S, val, y, nrhs, cnt, tk, status, st),
+        GLU_CUDA(solve_upper_trans(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "transposed upper solve");
+        GLU_CUDA(solve_lower_unit_trans(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st),
                  "transposed lower solve");
     }
     return GLU_OK;
@@ -458,8 +642,7 @@ Status solve_f32(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, 
     const TransformDev &T = h->T;
     GLU_CUDA(launch_transform_f32(trans ? T.tin_idx : T.in_idx, trans ? T.tin_scale : T.in_scale, bin, y,
                                   h->n, nrhs, st), "transform");
-    const float *val = h->d_val.as<float>() + size_t(inst) * h->nnz;
-    Status s = solve_inplace(h, val, y, nrhs, trans, st);
+    Status s = solve_inplace(h, inst, y, nrhs, trans, st);
     if (s != GLU_OK) return s;
     float *xout = (where == GLU_HOST) ? io : x;
     GLU_CUDA(launch_transform_f32(trans ? T.tout_idx : T.out_idx, trans ? T.tout_scale : T.out_scale, y,
@@ -763,14 +946,23 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         }
     }
     if (NL) GLU_CUDA(launch_scale_level(h->P, h->F, val, stride, count, pert, h->levels_h[NL - 1], st), "factor (scale)");
+    // dense trailing block: in place, or through the dense buffer
+    float *dbase = h->dense_buffer ? h->d_dense.as<float>() + size_t(first) * h->m * h->m : val;
+    const uint64_t dstride = h->dense_buffer ? uint64_t(h->m) * h->m : stride;
+    if (h->m && h->dense_buffer)
+        GLU_CUDA(launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
+                 "factor (dense gather)");
     for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
         uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
         uint32_t last_has_l = 0;  // the last column of the matrix has no L part
-        GLU_CUDA(launch_dense_panel(val, stride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
+        GLU_CUDA(launch_dense_panel(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
                                     h->d_diag_scratch.as<float>(), last_has_l, st), "factor (dense panel)");
-        GLU_CUDA(launch_dense_update(val, stride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
+        GLU_CUDA(launch_dense_update(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
                                      h->d_diag_scratch.as<float>(), st), "factor (dense update)");
     }
+    if (h->m && h->dense_buffer)
+        GLU_CUDA(launch_dense_scatter(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
+                 "factor (dense scatter)");
     GLU_CUDA(launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
     GLU_CUDA(cudaEventRecord(h->ev1, st), "event");
     uint32_t flags = 0;
@@ -850,13 +1042,12 @@ glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uin
             bz = b + off;
             xz = x + off;
         }
-        const float *val = h->d_val.as<float>() + size_t(z) * h->nnz;
         const double *ax0 = h->d_ax0.as<double>() + size_t(z) * h->nnz_src;
         GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
         GLU_CUDA(launch_norms(bz, n, nrhs, norms + 2 * nrhs, st), "norms");
         // x0 = solve(b)
         GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, bz, y, n, nrhs, st), "transform");
-        s = solve_inplace(h, val, y, nrhs, tr, st);
+        s = solve_inplace(h, z, y, nrhs, tr, st);
         if (s != GLU_OK) return s;
         GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 0, st), "transform");
         uint32_t it = 0;
@@ -878,7 +1069,7 @@ glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uin
             }
             if (worst2 <= tol || it >= maxit) break;
             GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, r, y, n, nrhs, st), "transform");
-            s = solve_inplace(h, val, y, nrhs, tr, st);
+            s = solve_inplace(h, z, y, nrhs, tr, st);
             if (s != GLU_OK) return s;
             GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 1, st), "transform");
         }
@@ -917,6 +1108,7 @@ glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t) {
     if (t->group_lanes && (t->group_lanes < 4 || t->group_lanes > 32 || (t->group_lanes & (t->group_lanes - 1))))
         return set_error(GLU_ERR_ARG, "group_lanes must be 0 or a power of two in [4, 32]");
     if (t->chain_cluster > 16) return set_error(GLU_ERR_ARG, "chain_cluster must be <= 16");
+    if (t->solve_cluster > 16) return set_error(GLU_ERR_ARG, "solve_cluster must be <= 16");
     DeviceGuard g(h->device);
     h->tune = *t;
     if (h->tune.chain_cluster) h->chain_cluster = h->tune.chain_cluster;

@@ -62,6 +62,112 @@ __device__ __forceinline__ void factor_diag_block(const float *__restrict__ val,
 // update kernel writes it back, so no block here overwrites an entry another
 // block may still read); blocks [1, 1+nL) compute rows of L21, the rest
 // columns of U12.  blockIdx.z selects the value set.
+// Full-width panel step (kb == kDenseNB), register resident: the diagonal
+// block is factored with every thread holding half a row (32 values) and the
+// pivot rows broadcast through shared memory, one barrier per column; the
+// L21 rows and U12 columns are then solved one per thread with the whole row
+// or column in registers.  Loops over columns are unrolled so that every
+// register index is static.
+__device__ __forceinline__ void factor_diag_regs(const float *__restrict__ val, const uint32_t *__restrict__ doff,
+                                                 uint32_t k0, uint32_t m, float pert, uint32_t last_has_l,
+                                                 float *sF, float (*urow)[kDenseNB]) {
+    constexpr int NB = kDenseNB;
+    constexpr int LD = kDenseNB + 1;
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t row = tid >> 1, half = tid & 1;
+    float a[32];
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) a[jj] = ld_cg(val + doff[k0 + half * 32 + jj] + k0 + row);
+#pragma unroll
+    for (int c = 0; c < NB; ++c) {
+        const int hc = c >> 5, jc = c & 31;
+        float *u = urow[c & 1];
+        if (row == uint32_t(c)) {
+            if (half == uint32_t(hc)) {
+                // a pivot is perturbed only when its column has an L part
+                const bool has_l = (k0 + c + 1 < m) || last_has_l;
+                float d = a[jc];
+                if (has_l && pert > 0.0f && fabsf(d) < pert) d = pert;
+                a[jc] = d;
+            }
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj)
+                if (int(half) * 32 + jj >= c) u[half * 32 + jj] = a[jj];
+        }
+        __syncthreads();
+        const float lsrc = __shfl_sync(0xffffffffu, a[jc], (lane & ~1u) | uint32_t(hc));
+        if (row > uint32_t(c)) {
+            const float l = lsrc / u[c];
+            if (half == uint32_t(hc)) a[jc] = l;
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj)
+                if (int(half) * 32 + jj > c) a[jj] = fmaf(-l, u[half * 32 + jj], a[jj]);
+        }
+    }
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) sF[(half * 32 + jj) * LD + row] = a[jj];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPanelRows, 3) k_dense_panel_full(float *val_base, uint64_t stride,
+                                                                    const uint32_t *__restrict__ doff, uint32_t m,
+                                                                    uint32_t k0, const float *pert_z,
+                                                                    float *diag_scratch, uint32_t last_has_l,
+                                                                    uint32_t nL) {
+    constexpr int NB = kDenseNB;
+    constexpr int LD = kDenseNB + 1;
+    __shared__ float sF[NB * LD];
+    __shared__ float urow[2][NB];
+    float *val = val_base + blockIdx.z * stride;
+    const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
+    factor_diag_regs(val, doff, k0, m, pert, last_has_l, sF, urow);
+    const uint32_t r0 = k0 + NB;
+    const uint32_t tid = threadIdx.x;
+    if (blockIdx.x == 0) {
+        float *ds = diag_scratch + size_t(blockIdx.z) * NB * NB;
+        for (uint32_t e = tid; e < NB * NB; e += blockDim.x) {
+            uint32_t c = e / NB, r = e - c * NB;
+            ds[c * NB + r] = sF[c * LD + r];
+        }
+        return;
+    }
+    float a[NB];
+    if (blockIdx.x <= nL) {
+        // row of L21: x U11 = a
+        const uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
+        if (r >= m) return;
+#pragma unroll
+        for (int c = 0; c < NB; ++c) a[c] = ld_cg(val + doff[k0 + c] + r);
+#pragma unroll
+        for (int c = 0; c < NB; ++c) {
+            const float l = a[c] / sF[c * LD + c];
+            a[c] = l;
+#pragma unroll
+            for (int j = c + 1; j < NB; ++j) a[j] = fmaf(-l, sF[j * LD + c], a[j]);
+        }
+#pragma unroll
+        for (int c = 0; c < NB; ++c) st_cg(val + doff[k0 + c] + r, a[c]);
+    } else {
+        // column of U12: L11 x = a
+        const uint32_t j = r0 + (blockIdx.x - 1 - nL) * kPanelRows + tid;
+        if (j >= m) return;
+        float *col = val + doff[j] + k0;
+#pragma unroll
+        for (int r = 0; r < NB; ++r) a[r] = ld_cg(col + r);
+#pragma unroll
+        for (int r = 0; r < NB; ++r) {
+            const float u = a[r];
+#pragma unroll
+            for (int i = r + 1; i < NB; ++i) a[i] = fmaf(-sF[r * LD + i], u, a[i]);
+        }
+#pragma unroll
+        for (int r = 0; r < NB; ++r) st_cg(col + r, a[r]);
+    }
+}
+
+constexpr int kPW = kPanelRows + 1;  // leading dimension of the panel work tile
+constexpr size_t kPanelSmem = sizeof(float) * (size_t(kDenseNB) * (kDenseNB + 1) + kDenseNB + size_t(kDenseNB) * kPW);
+
 __global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uint64_t stride,
                                                             const uint32_t *__restrict__ doff,
                                                             uint32_t m, uint32_t k0, uint32_t kb,
@@ -69,8 +175,10 @@ __global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uin
                                                             uint32_t last_has_l, uint32_t nL) {
     constexpr int NB = kDenseNB;
     constexpr int LD = kDenseNB + 1;
-    __shared__ float sF[NB * LD];
-    __shared__ float lcol[NB];
+    extern __shared__ float4 psm4[];
+    float *sF = reinterpret_cast<float *>(psm4);  // diagonal block, column-major
+    float *lcol = sF + NB * LD;                   // multipliers of the current step
+    float *sW = lcol + NB;                        // [k][thread]: rows of L21 or columns of U12
     float *val = val_base + blockIdx.z * stride;
     float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
     factor_diag_block(val, doff, k0, kb, m, pert, last_has_l, sF, lcol);
@@ -85,42 +193,39 @@ __global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uin
         return;
     }
     if (blockIdx.x <= nL) {
-        // row of L21: x U11 = a
-        uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
+        // row of L21, one per thread: x U11 = a, in the thread's slot of sW
+        const uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
         if (r >= m) return;
-        float a[NB];
-#pragma unroll
-        for (int c = 0; c < NB; ++c) a[c] = (c < (int)kb) ? ld_cg(val + doff[k0 + c] + r) : 0.0f;
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if (c < (int)kb) {
-                float l = a[c] / sF[c * LD + c];
-                a[c] = l;
-#pragma unroll
-                for (int j = c + 1; j < NB; ++j) a[j] -= l * sF[j * LD + c];
+        float *w = sW + tid;
+        for (uint32_t c = 0; c < kb; ++c) w[c * kPW] = ld_cg(val + doff[k0 + c] + r);
+        for (uint32_t c = 0; c < kb; ++c) {
+            const float l = w[c * kPW] / sF[c * LD + c];
+            w[c * kPW] = l;
+            for (uint32_t j = c + 1; j < kb; ++j) w[j * kPW] -= l * sF[j * LD + c];
+        }
+        for (uint32_t c = 0; c < kb; ++c) st_cg(val + doff[k0 + c] + r, w[c * kPW]);
+    } else {
+        // column of U12, one per thread: L11 x = a (loaded and stored with
+        // consecutive threads on consecutive rows of one column)
+        const uint32_t j0 = r0 + (blockIdx.x - 1 - nL) * kPanelRows;
+        const uint32_t ncol = min(uint32_t(kPanelRows), m - j0);
+        for (uint32_t e = tid; e < ncol * kb; e += blockDim.x) {
+            uint32_t cc = e / kb, rr = e - cc * kb;
+            sW[rr * kPW + cc] = ld_cg(val + doff[j0 + cc] + k0 + rr);
+        }
+        __syncthreads();
+        if (tid < ncol) {
+            float *w = sW + tid;
+            for (uint32_t rr = 0; rr < kb; ++rr) {
+                const float u = w[rr * kPW];
+                for (uint32_t i = rr + 1; i < kb; ++i) w[i * kPW] -= sF[rr * LD + i] * u;
             }
         }
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-            if (c < (int)kb) st_cg(val + doff[k0 + c] + r, a[c]);
-    } else {
-        // column of U12: L11 x = a
-        uint32_t j = r0 + (blockIdx.x - 1 - nL) * kPanelRows + tid;
-        if (j >= m) return;
-        const float *col = val + doff[j] + k0;
-        float a[NB];
-#pragma unroll
-        for (int r = 0; r < NB; ++r) a[r] = (r < (int)kb) ? ld_cg(col + r) : 0.0f;
-#pragma unroll
-        for (int r = 0; r < NB; ++r) {
-            float u = a[r];
-#pragma unroll
-            for (int i = r + 1; i < NB; ++i) a[i] -= sF[r * LD + i] * u;
+        __syncthreads();
+        for (uint32_t e = tid; e < ncol * kb; e += blockDim.x) {
+            uint32_t cc = e / kb, rr = e - cc * kb;
+            st_cg(val + doff[j0 + cc] + k0 + rr, sW[rr * kPW + cc]);
         }
-        float *colw = val + doff[j] + k0;
-#pragma unroll
-        for (int r = 0; r < NB; ++r)
-            if (r < (int)kb) st_cg(colw + r, a[r]);
     }
 }
 
@@ -161,7 +266,8 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     const uint32_t tx = tid & 15, ty = tid >> 4;
     // C tile into registers (through shared memory for coalescing): every
     // entry then receives its updates one k at a time, in increasing k, as in
-    // the column algorithm.
+    // the column algorithm.  (Loops unrolled so that many loads are in flight.)
+#pragma unroll 16
     for (uint32_t e = tid; e < uint32_t(kTB) * kTB; e += 256) {
         uint32_t col = e / kTB, row = e - col * kTB;
         float v = 0.0f;
@@ -176,6 +282,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
         for (int i = 0; i < 8; ++i) acc[i][j] = sC[(tx * 8 + j) * kLDC + ty * 8 + i];
     __syncthreads();
     // stage L21 tile: sA[k][row]
+#pragma unroll 16
     for (uint32_t e = tid; e < uint32_t(kDenseNB) * kTB; e += 256) {
         uint32_t k = e / kTB, row = e - k * kTB;
         float v = 0.0f;
@@ -185,6 +292,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
     {
         uint32_t lane = tid & 31, w = tid >> 5;
+#pragma unroll 8
         for (uint32_t col = w; col < uint32_t(kTB); col += 8) {
             bool cok = cbase + col < mp;
             const float *src = cok ? val + doff[r0 + cbase + col] + k0 : nullptr;
@@ -226,12 +334,22 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
 cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
                                float *diag_scratch, uint32_t last_has_l, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_dense_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(kPanelSmem));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
     uint32_t rest = m - (k0 + kb);
     uint32_t nL = (rest + kPanelRows - 1) / kPanelRows;
     uint32_t nU = nL;
     dim3 grid(1 + nL + nU, 1, count);
-    k_dense_panel<<<grid, kPanelRows, 0, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
-                                               last_has_l, nL);
+    if (kb == uint32_t(kDenseNB))
+        k_dense_panel_full<<<grid, kPanelRows, 0, st>>>(val, stride, doff, m, k0, pert_z, diag_scratch, last_has_l, nL);
+    else
+        k_dense_panel<<<grid, kPanelRows, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
+                                                            last_has_l, nL);
     return cudaGetLastError();
 }
 
@@ -250,6 +368,47 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
     if (tiles == 0) tiles = 1;
     dim3 grid(tiles, tiles, count);
     k_dense_update<<<grid, 256, kUpdateSmem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------ dense buffer gather/scatter --
+// One warp per tail column; blockIdx.z selects the value set.
+__global__ void __launch_bounds__(256) k_dense_gather(DevPattern P, const float *__restrict__ val_base,
+                                                      uint64_t stride, uint32_t t, uint32_t m,
+                                                      const uint32_t *__restrict__ tail_start, float *dbuf) {
+    const float *val = val_base + blockIdx.z * stride;
+    float *D = dbuf + size_t(blockIdx.z) * m * m;
+    const uint32_t j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= m) return;
+    float *col = D + size_t(j) * m;
+    for (uint32_t p = tail_start[j] + lane; p < P.cptr[t + j + 1]; p += 32) col[P.ridx[p] - t] = val[p];
+}
+
+__global__ void __launch_bounds__(256) k_dense_scatter(DevPattern P, float *val_base, uint64_t stride,
+                                                       uint32_t t, uint32_t m,
+                                                       const uint32_t *__restrict__ tail_start,
+                                                       const float *__restrict__ dbuf) {
+    float *val = val_base + blockIdx.z * stride;
+    const float *D = dbuf + size_t(blockIdx.z) * m * m;
+    const uint32_t j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (j >= m) return;
+    const float *col = D + size_t(j) * m;
+    for (uint32_t p = tail_start[j] + lane; p < P.cptr[t + j + 1]; p += 32) val[p] = col[P.ridx[p] - t];
+}
+
+cudaError_t launch_dense_gather(const DevPattern &P, const float *val, uint64_t stride, uint32_t count,
+                                uint32_t t, uint32_t m, const uint32_t *tail_start, float *dbuf,
+                                cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(dbuf, 0, sizeof(float) * size_t(m) * m * count, st);
+    if (e != cudaSuccess) return e;
+    k_dense_gather<<<dim3((m + 7) / 8, 1, count), 256, 0, st>>>(P, val, stride, t, m, tail_start, dbuf);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_scatter(const DevPattern &P, float *val, uint64_t stride, uint32_t count,
+                                 uint32_t t, uint32_t m, const uint32_t *tail_start, const float *dbuf,
+                                 cudaStream_t st) {
+    k_dense_scatter<<<dim3((m + 7) / 8, 1, count), 256, 0, st>>>(P, val, stride, t, m, tail_start, dbuf);
     return cudaGetLastError();
 }
 

@@ -51,6 +51,18 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
 cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
                                 cudaStream_t st);
+// A trailing block that is dense but not completely filled is factored in a
+// separate m x m column-major buffer: gather copies the block's pattern
+// entries of the CSC values into the (zeroed) buffer, scatter copies the
+// factored entries back.  Entries outside the pattern stay exactly zero
+// through the factorization.  tail_start[j] = CSC position of the first row
+// >= t in column t + j.
+cudaError_t launch_dense_gather(const DevPattern &P, const float *val, uint64_t stride, uint32_t count,
+                                uint32_t t, uint32_t m, const uint32_t *tail_start, float *dbuf,
+                                cudaStream_t st);
+cudaError_t launch_dense_scatter(const DevPattern &P, float *val, uint64_t stride, uint32_t count,
+                                 uint32_t t, uint32_t m, const uint32_t *tail_start, const float *dbuf,
+                                 cudaStream_t st);
 
 // -------------------------------------------------------------- utilities --
 // pert[z] = 3.45e-4 * max_col sum |val| (FP32, column order), numeric.cu:490-506.
@@ -73,12 +85,35 @@ cudaError_t build_levels(const DevPattern &P, void *scratch, int32_t *level_of, 
                          cudaStream_t st);
 
 // ------------------------------------------------------------------ solves --
+// Level schedule of one sparse sweep over the columns [0, t): the columns
+// level by level (cols, lptr on the device) and the launches that run them.
+// A step is one level with its own launch (kind 0, columns [c0, c1) of cols)
+// or a run of thin levels [l0, l1) inside one thread-block cluster (kind 1).
+// Every sweep is in scatter form: once x_j is final, its column (L, U: CSC)
+// or row (U^T, L^T: CSR) is subtracted from the other unknowns.  Work items
+// are (j, chunk of kSweepChunk entries); item_off is their prefix over cols.
+struct SweepStep {
+    uint32_t kind, l0, l1, s0, s1;  // levels [l0, l1), columns cols[s0, s1)
+};
+struct SweepPlan {
+    const uint32_t *cols = nullptr;
+    const uint32_t *lptr = nullptr;
+    const uint32_t *item_off = nullptr;
+    const SweepStep *steps = nullptr;  // host array
+    uint32_t nsteps = 0;
+    uint32_t nlev = 0;
+};
+enum SweepMode : int { SWEEP_L = 0, SWEEP_U = 1, SWEEP_UT = 2, SWEEP_LT = 3 };
+constexpr uint32_t kSweepChunk = 128;
+
 struct SolvePlanDev {
-    uint32_t t;                 // first column of the dense tail (n if none)
-    uint32_t m;                 // order of the dense tail
-    const uint32_t *doff;       // dense tail column offsets
-    const uint32_t *l_indeg;    // CSR entries left of the diagonal per row (L in-degree)
-    const uint32_t *u_indeg;    // CSR entries right of the diagonal per row (U in-degree)
+    uint32_t t;                     // first column of the dense tail (n if none)
+    uint32_t m;                     // order of the dense tail
+    const uint32_t *doff;           // dense tail column offsets (into the dense view)
+    const uint32_t *tail_start;     // CSC position of the first row >= t of each tail column
+    const uint32_t *tail_row_start; // CSR position of the first column >= t of each tail row
+    SweepPlan sweep[4];             // L, U, U^T, L^T
+    uint32_t cluster;               // CTAs of the thin-level cluster kernel
 };
 
 // Transform in: y[j] = rhs[col_perm[piv[j]]] * (mc64 ? col_scale_perm[piv[j]] : 1)
@@ -95,20 +130,24 @@ struct TransformDev {
     const double *tout_scale;
 };
 
-// FP32 triangular solves on y (nrhs vectors of n, one after another), in place.
+constexpr uint32_t kSolveChainThreads = 512;
+// FP32 triangular solves on y (nrhs vectors of n, one after another), in
+// place.  val: CSC factor values; dval: base of the dense tail view.
+// xo: n * nrhs floats of scratch (finished values of the dividing sweeps);
+// counters / ticket: scratch of the dense tail sweeps.
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                             float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                             uint32_t *status, cudaStream_t st);
-cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y,
-                        uint32_t nrhs, uint32_t *counters, uint32_t *ticket, uint32_t *status,
-                        cudaStream_t st);
+                             const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                             uint32_t *ticket, uint32_t *status, cudaStream_t st);
+cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val,
+                        const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                        uint32_t *ticket, uint32_t *status, cudaStream_t st);
 // Transposed: U^T z = y (forward), then L^T w = z (backward).
 cudaError_t solve_upper_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                              float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                              uint32_t *status, cudaStream_t st);
+                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                              uint32_t *ticket, uint32_t *status, cudaStream_t st);
 cudaError_t solve_lower_unit_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                                   float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                                   uint32_t *status, cudaStream_t st);
+                                   const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                                   uint32_t *ticket, uint32_t *status, cudaStream_t st);
 
 // Permute/scale kernels of the solve transforms.
 cudaError_t launch_transform_f32(const uint32_t *idx, const double *scale, const float *in,

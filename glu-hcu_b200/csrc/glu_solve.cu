@@ -5,21 +5,25 @@
 // U column sweep with the diagonal divide (:232-239), permute/scale back.
 // Here the same sweeps run on the GPU:
 //
-//  * sparse columns (in front of the dense trailing block) are processed
-//    sync-free: one warp per column, claimed in dependency order through an
-//    atomic ticket, waits (bounded) until every column it depends on has
-//    finished, then scatters its updates (L, U: atomics plus a per-row
-//    completion counter) or gathers them (L^T, U^T: dot products behind
-//    per-column done flags);
+//  * sparse columns (in front of the dense trailing block) are processed level
+//    by level, with level sets of each sweep's own dependency graph computed
+//    once per pattern: a level with many columns gets its own launch (one warp
+//    per column); a run of thin levels executes inside one thread-block
+//    cluster that steps from level to level with hardware cluster barriers.
+//    L and U sweeps scatter (x_i -= L(i,j) x_j with atomics), the transposed
+//    sweeps gather (dot products, no atomics);
 //  * the dense trailing block is solved by row blocks of 64: a block adds the
 //    contribution of every finished earlier block (one 64 x 64 tile each,
 //    staged in shared memory) and then solves its diagonal tile; blocks are
-//    claimed in order through a ticket and wait (bounded) on per-block flags.
-//
-// Every wait gives up after kSpinLimit polls and sets DEV_TIMEOUT, so a
-// broken dependency can never hang the device.
+//    claimed in order through a ticket and wait (bounded) on per-block flags;
+//  * the coupling between the two (U entries of tail columns in sparse rows)
+//    is one parallel scatter or gather over the tail columns.
+#include <cooperative_groups.h>
+
 #include "glu_common.cuh"
 #include "glu_kernels.h"
+
+namespace cg = cooperative_groups;
 
 namespace glu {
 
@@ -38,139 +42,158 @@ __device__ __forceinline__ bool wait_count(const uint32_t *cnt, uint32_t target,
 }
 
 // ------------------------------------------------------------ sparse sweeps --
-// Forward unit-L sweep over columns [0, t) in scatter form: x_i -= L(i,j) x_j.
-// need[i] = number of columns c < min(i, t) with L(i,c) != 0.
-__global__ void __launch_bounds__(256) k_sparse_lower(DevPattern P, uint32_t t, const float *__restrict__ val,
-                                                      float *y, uint32_t nrhs, const uint32_t *need,
-                                                      uint32_t *cnt, uint32_t *ticket, uint32_t *status) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t j = 0;
-    if (lane == 0) j = atomicAdd(ticket, 1u);
-    j = __shfl_sync(0xffffffffu, j, 0);
-    if (j >= t) return;
-    if (lane == 0) wait_count(cnt + j, need[j], status);
-    __syncwarp();
-    const uint32_t n = P.n;
-    const uint32_t l0 = P.diag[j] + 1, l1 = P.cptr[j + 1];
-    for (uint32_t r = 0; r < nrhs; ++r) {
-        float xj = __ldcg(y + size_t(r) * n + j);
-        if (xj == 0.0f) continue;
-        for (uint32_t p = l0 + lane; p < l1; p += 32)
-            atomicAdd(y + size_t(r) * n + P.ridx[p], -__fmul_rn(val[p], xj));
-    }
-    __threadfence();
-    for (uint32_t p = l0 + lane; p < l1; p += 32) atomicAdd(cnt + P.ridx[p], 1u);
-}
-
-// Backward U sweep in scatter form, columns claimed from n-1 down.  Columns of
-// the dense tail ([t, n)) are already solved: they only scatter their U rows
-// that lie above t.  need[r] = number of columns c > r with U(r,c) != 0.
-__global__ void __launch_bounds__(256) k_sparse_upper(DevPattern P, uint32_t t, const uint32_t *__restrict__ doff,
-                                                      const float *__restrict__ val, float *y, uint32_t nrhs,
-                                                      const uint32_t *need, uint32_t *cnt, uint32_t *ticket,
-                                                      uint32_t *status) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t tk = 0;
-    if (lane == 0) tk = atomicAdd(ticket, 1u);
-    tk = __shfl_sync(0xffffffffu, tk, 0);
-    const uint32_t n = P.n;
-    if (tk >= n) return;
-    const uint32_t j = n - 1 - tk;
-    const uint32_t u0 = P.cptr[j];
-    uint32_t u1;
-    if (j >= t) {
-        u1 = doff[j - t];  // rows < t of a tail column
+// Every sweep is in scatter form: once x_j is final, the entries of its
+//   SWEEP_L : CSC column j below the diagonal   (x_j = y_j)
+//   SWEEP_U : CSC column j above the diagonal   (x_j = y_j / U(j,j))
+//   SWEEP_UT: CSR row j right of the diagonal    (x_j = y_j / U(j,j))
+//   SWEEP_LT: CSR row j left of the diagonal     (x_j = y_j)
+// are subtracted: y_target -= entry * x_j.  A long column or row is split into
+// items of kSweepChunk entries that run in parallel; every item of j reads
+// the same y_j (nothing writes y_j while its level runs) and the dividing
+// sweeps store the finished x_j to xo (item 0 of j).
+template <int kMode>
+__device__ __forceinline__ void sweep_item(const DevPattern &P, const float *__restrict__ val, float *y, float *xo,
+                                           uint32_t nrhs, const uint32_t *__restrict__ cols,
+                                           const uint32_t *__restrict__ item_off, uint32_t s0, uint32_t s1,
+                                           uint32_t it, uint32_t lane) {
+    constexpr bool kDiv = (kMode == SWEEP_U || kMode == SWEEP_UT);
+    constexpr bool kRow = (kMode == SWEEP_UT || kMode == SWEEP_LT);
+    const uint32_t s = upper_slot(item_off, s0, s1, it);
+    const uint32_t j = cols[s];
+    const uint32_t rem = it - item_off[s];
+    uint32_t p0, p1;
+    if (kMode == SWEEP_L) {
+        p0 = P.diag[j] + 1;
+        p1 = P.cptr[j + 1];
+    } else if (kMode == SWEEP_U) {
+        p0 = P.cptr[j];
+        p1 = P.diag[j];
+    } else if (kMode == SWEEP_UT) {
+        p0 = P.rdiag[j] + 1;
+        p1 = P.rptr[j + 1];
     } else {
-        u1 = P.diag[j];
-        if (lane == 0) wait_count(cnt + j, need[j], status);
-        __syncwarp();
-        const float d = val[P.diag[j]];
-        for (uint32_t r = lane; r < nrhs; r += 32) {
-            float *pj = y + size_t(r) * n + j;
-            __stcg(pj, __ldcg(pj) / d);
-        }
-        __syncwarp();
-        __threadfence_block();
+        p0 = P.rptr[j];
+        p1 = P.rdiag[j];
     }
+    const uint32_t e0 = p0 + rem * kSweepChunk;
+    const uint32_t e1 = min(e0 + kSweepChunk, p1);
+    const uint32_t n = P.n;
+    const float d = kDiv ? val[P.diag[j]] : 1.0f;
     for (uint32_t r = 0; r < nrhs; ++r) {
-        float xj = __ldcg(y + size_t(r) * n + j);
+        float *yr = y + size_t(r) * n;
+        float xj = __ldcg(yr + j);
+        if (kDiv) {
+            xj = xj / d;
+            if (rem == 0 && lane == 0) xo[size_t(r) * n + j] = xj;
+        }
         if (xj == 0.0f) continue;
-        for (uint32_t p = u0 + lane; p < u1; p += 32)
-            atomicAdd(y + size_t(r) * n + P.ridx[p], -__fmul_rn(val[p], xj));
-    }
-    __threadfence();
-    for (uint32_t p = u0 + lane; p < u1; p += 32) atomicAdd(cnt + P.ridx[p], 1u);
-}
-
-// Forward U^T sweep over columns [0, t) in gather form:
-// z_j = (y_j - sum_{i<j} U(i,j) z_i) / U(j,j).  done[i] = 1 when z_i is final.
-// For tail columns (j >= t) only the part over rows i < t is subtracted here.
-__global__ void __launch_bounds__(256) k_sparse_upper_trans(DevPattern P, uint32_t t, const uint32_t *__restrict__ doff,
-                                                            const float *__restrict__ val, float *y,
-                                                            uint32_t nrhs, uint32_t *done, uint32_t *ticket,
-                                                            uint32_t *status) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t j = 0;
-    if (lane == 0) j = atomicAdd(ticket, 1u);
-    j = __shfl_sync(0xffffffffu, j, 0);
-    const uint32_t n = P.n;
-    if (j >= n) return;
-    const uint32_t u0 = P.cptr[j];
-    const uint32_t u1 = (j >= t) ? doff[j - t] : P.diag[j];
-    for (uint32_t p = u0 + lane; p < u1; p += 32) wait_count(done + P.ridx[p], 1u, status);
-    __syncwarp();
-    for (uint32_t r = 0; r < nrhs; ++r) {
-        float acc = 0.0f;
-        for (uint32_t p = u0 + lane; p < u1; p += 32)
-            acc = fmaf(val[p], __ldcg(y + size_t(r) * n + P.ridx[p]), acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) {
-            float *pj = y + size_t(r) * n + j;
-            float v = __ldcg(pj) - acc;
-            if (j < t) v = v / val[P.diag[j]];
-            __stcg(pj, v);
+        for (uint32_t e = e0 + lane; e < e1; e += 32) {
+            const uint32_t tgt = kRow ? P.cidx[e] : P.ridx[e];
+            const float v = kRow ? val[P.cpos[e]] : val[e];
+            atomicAdd(yr + tgt, -__fmul_rn(v, xj));
         }
-    }
-    __syncwarp();
-    if (lane == 0 && j < t) {
-        __threadfence();
-        st_release_gpu(done + j, 1u);
     }
 }
 
-// Backward L^T sweep over columns [0, t) in gather form (tail already done):
-// w_j = z_j - sum_{i>j} L(i,j) w_i, columns claimed from t-1 down.
-__global__ void __launch_bounds__(256) k_sparse_lower_trans(DevPattern P, uint32_t t, const float *__restrict__ val,
-                                                            float *y, uint32_t nrhs, uint32_t *done,
-                                                            uint32_t *ticket, uint32_t *status) {
+// One level, own launch: warps over the items of cols[s0, s1).
+template <int kMode>
+__global__ void __launch_bounds__(256) k_sweep_level(DevPattern P, const float *__restrict__ val, float *y, float *xo,
+                                                     uint32_t nrhs, const uint32_t *__restrict__ cols,
+                                                     const uint32_t *__restrict__ item_off, uint32_t s0,
+                                                     uint32_t s1) {
     const uint32_t lane = threadIdx.x & 31;
-    uint32_t tk = 0;
-    if (lane == 0) tk = atomicAdd(ticket, 1u);
-    tk = __shfl_sync(0xffffffffu, tk, 0);
-    if (tk >= t) return;
-    const uint32_t j = t - 1 - tk;
-    const uint32_t n = P.n;
-    const uint32_t l0 = P.diag[j] + 1, l1 = P.cptr[j + 1];
-    for (uint32_t p = l0 + lane; p < l1; p += 32) {
-        uint32_t i = P.ridx[p];
-        if (i < t) wait_count(done + i, 1u, status);
+    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    const uint32_t it0 = item_off[s0], it1 = item_off[s1];
+    for (uint32_t it = it0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < it1; it += nw)
+        sweep_item<kMode>(P, val, y, xo, nrhs, cols, item_off, s0, s1, it, lane);
+}
+
+// A run of thin levels [l0, l1) inside one cluster; cluster barrier between
+// levels; values of y written by other blocks are read through L2.
+template <int kMode>
+__global__ void __launch_bounds__(kSolveChainThreads) k_sweep_chain(DevPattern P, const float *__restrict__ val,
+                                                                    float *y, float *xo, uint32_t nrhs,
+                                                                    const uint32_t *__restrict__ cols,
+                                                                    const uint32_t *__restrict__ lptr,
+                                                                    const uint32_t *__restrict__ item_off,
+                                                                    uint32_t l0, uint32_t l1) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const uint32_t nblk = cluster.num_blocks();
+    const uint32_t rank = cluster.block_rank();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t w0 = rank * wpb + (threadIdx.x >> 5), nw = nblk * wpb;
+    for (uint32_t l = l0; l < l1; ++l) {
+        const uint32_t s0 = lptr[l], s1 = lptr[l + 1];
+        const uint32_t it0 = item_off[s0], it1 = item_off[s1];
+        for (uint32_t it = it0 + w0; it < it1; it += nw) sweep_item<kMode>(P, val, y, xo, nrhs, cols, item_off, s0, s1, it, lane);
+        cluster.sync();
     }
-    __syncwarp();
+}
+
+// Coupling of the dense tail with the sparse unknowns, one warp per tail
+// column / row j (x_j final): y_i -= U(i,j) x_j for the U entries of tail
+// column j in rows i < t (kRow = false, before the sparse U sweep), or
+// y_c -= L(j,c) x_j for the L entries of tail row j in columns c < t
+// (kRow = true, before the sparse L^T sweep).
+template <bool kRow>
+__global__ void __launch_bounds__(256) k_tail_coupling(DevPattern P, uint32_t t, uint32_t m,
+                                                       const uint32_t *__restrict__ tail_start,
+                                                       const float *__restrict__ val, float *y, uint32_t nrhs) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t jj = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (jj >= m) return;
+    const uint32_t j = t + jj, n = P.n;
+    const uint32_t p0 = kRow ? P.rptr[j] : P.cptr[j], p1 = tail_start[jj];
     for (uint32_t r = 0; r < nrhs; ++r) {
-        float acc = 0.0f;
-        for (uint32_t p = l0 + lane; p < l1; p += 32)
-            acc = fmaf(val[p], __ldcg(y + size_t(r) * n + P.ridx[p]), acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) {
-            float *pj = y + size_t(r) * n + j;
-            __stcg(pj, __ldcg(pj) - acc);
+        float *yr = y + size_t(r) * n;
+        const float xj = yr[j];
+        if (xj == 0.0f) continue;
+        for (uint32_t p = p0 + lane; p < p1; p += 32) {
+            const uint32_t tgt = kRow ? P.cidx[p] : P.ridx[p];
+            const float v = kRow ? val[P.cpos[p]] : val[p];
+            atomicAdd(yr + tgt, -__fmul_rn(v, xj));
         }
     }
-    __syncwarp();
-    if (lane == 0) {
-        __threadfence();
-        st_release_gpu(done + j, 1u);
+}
+
+// y[j] = xo[j] for the sparse unknowns j < t (after a dividing sweep).
+__global__ void k_copy_sparse(const float *__restrict__ xo, float *y, uint32_t t, uint32_t n) {
+    const size_t off = size_t(blockIdx.y) * n;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < t; j += gridDim.x * blockDim.x) y[off + j] = xo[off + j];
+}
+
+template <int kMode>
+static cudaError_t run_sweep(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y, float *xo,
+                             uint32_t nrhs, cudaStream_t st) {
+    const SweepPlan &sw = S.sweep[kMode];
+    for (uint32_t i = 0; i < sw.nsteps; ++i) {
+        const SweepStep &s = sw.steps[i];
+        if (s.kind == 0) {
+            k_sweep_level<kMode><<<148 * 8, 256, 0, st>>>(P, val, y, xo, nrhs, sw.cols, sw.item_off, s.s0, s.s1);
+        } else {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(S.cluster, 1, 1);
+            cfg.blockDim = dim3(kSolveChainThreads, 1, 1);
+            cfg.stream = st;
+            cudaLaunchAttribute attr[1];
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = S.cluster;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+            cudaError_t e = cudaLaunchKernelEx(&cfg, k_sweep_chain<kMode>, P, val, y, xo, nrhs, sw.cols, sw.lptr,
+                                               sw.item_off, s.l0, s.l1);
+            if (e != cudaSuccess) return e;
+        }
     }
+    if ((kMode == SWEEP_U || kMode == SWEEP_UT) && S.t > 0) {
+        uint32_t bx = (S.t + 255) / 256;
+        if (bx > 1024) bx = 1024;
+        k_copy_sparse<<<dim3(bx, nrhs, 1), 256, 0, st>>>(xo, y, S.t, P.n);
+    }
+    return cudaGetLastError();
 }
 
 // --------------------------------------------------------- dense tail sweeps --
@@ -221,7 +244,13 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
             for (uint32_t e = tid; e < kRB * kRB; e += 256) {
                 uint32_t a = e / kRB, bb = e % kRB;  // coalesced along bb
                 uint32_t i, cc;
-                if (kTrans) { i = a; cc = bb; } else { cc = a; i = bb; }
+                if (kTrans) {
+                    i = a;
+                    cc = bb;
+                } else {
+                    cc = a;
+                    i = bb;
+                }
                 float v = 0.0f;
                 if (rb0 + i < rb1 && cb0 + cc < cb1) v = T(rb0 + i, cb0 + cc);
                 tile[i][cc] = v;
@@ -247,7 +276,13 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
         for (uint32_t e = tid; e < kRB * kRB; e += 256) {
             uint32_t a = e / kRB, bb = e % kRB;
             uint32_t i, cc;
-            if (kTrans) { i = a; cc = bb; } else { cc = a; i = bb; }
+            if (kTrans) {
+                i = a;
+                cc = bb;
+            } else {
+                cc = a;
+                i = bb;
+            }
             float v = 0.0f;
             if (rb0 + i < rb1 && rb0 + cc < rb1) v = T(rb0 + i, rb0 + cc);
             tile[i][cc] = v;
@@ -258,17 +293,21 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
         if (w < nr) {
             const uint32_t r = w;
             float v0 = 0.f, v1 = 0.f;  // rows lane and lane+32
-            if (lane < rows) v0 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane) -
-                                  (part[0][lane][r] + part[1][lane][r] + part[2][lane][r] + part[3][lane][r]);
-            if (lane + 32 < rows) v1 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane + 32) -
-                                       (part[0][lane + 32][r] + part[1][lane + 32][r] + part[2][lane + 32][r] +
-                                        part[3][lane + 32][r]);
+            if (lane < rows)
+                v0 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane) -
+                     (part[0][lane][r] + part[1][lane][r] + part[2][lane][r] + part[3][lane][r]);
+            if (lane + 32 < rows)
+                v1 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane + 32) -
+                     (part[0][lane + 32][r] + part[1][lane + 32][r] + part[2][lane + 32][r] + part[3][lane + 32][r]);
             for (uint32_t s = 0; s < rows; ++s) {
                 const uint32_t c = kLower ? s : rows - 1 - s;
                 float xc = __shfl_sync(0xffffffffu, c < 32 ? v0 : v1, c & 31);
                 if (!kUnit) xc = xc / tile[c][c];
                 if (lane == (c & 31)) {
-                    if (c < 32) v0 = xc; else v1 = xc;
+                    if (c < 32)
+                        v0 = xc;
+                    else
+                        v1 = xc;
                 }
                 // update the rows still to solve
                 uint32_t i0 = lane, i1 = lane + 32;
@@ -289,7 +328,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
 }
 
 template <int kMode>
-static cudaError_t dense_sweep(const SolvePlanDev &S, const float *val, float *y, uint32_t n,
+static cudaError_t dense_sweep(const SolvePlanDev &S, const float *dval, float *y, uint32_t n,
                                uint32_t nrhs, uint32_t *flags, uint32_t *ticket, uint32_t *status,
                                cudaStream_t st) {
     if (S.m == 0) return cudaSuccess;
@@ -297,69 +336,52 @@ static cudaError_t dense_sweep(const SolvePlanDev &S, const float *val, float *y
     cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * nb, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_dense_trsv<kMode><<<nb, 256, 0, st>>>(val, S.doff, S.t, S.m, y, n, nrhs, flags, ticket, status);
+    k_dense_trsv<kMode><<<nb, 256, 0, st>>>(dval, S.doff, S.t, S.m, y, n, nrhs, flags, ticket, status);
     return cudaGetLastError();
 }
 
-static cudaError_t reset(uint32_t *counters, uint32_t n, uint32_t *ticket, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(uint32_t) * n, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
-    return e;
+static cudaError_t tail_coupling(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y,
+                                 uint32_t nrhs, bool rows, cudaStream_t st) {
+    if (S.m == 0 || S.t == 0) return cudaSuccess;
+    uint32_t blocks = (S.m + 7) / 8;
+    if (rows)
+        k_tail_coupling<true><<<blocks, 256, 0, st>>>(P, S.t, S.m, S.tail_row_start, val, y, nrhs);
+    else
+        k_tail_coupling<false><<<blocks, 256, 0, st>>>(P, S.t, S.m, S.tail_start, val, y, nrhs);
+    return cudaGetLastError();
 }
-
-static inline uint32_t warp_blocks(uint32_t warps) { return (warps + 7) / 8; }
 
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                             float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                             uint32_t *status, cudaStream_t st) {
-    cudaError_t e;
-    if (S.t > 0) {
-        if ((e = reset(counters, P.n, ticket, st)) != cudaSuccess) return e;
-        k_sparse_lower<<<warp_blocks(S.t), 256, 0, st>>>(P, S.t, val, y, nrhs, S.l_indeg, counters,
-                                                         ticket, status);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    return dense_sweep<0>(S, val, y, P.n, nrhs, counters, ticket, status, st);
+                             const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                             uint32_t *ticket, uint32_t *status, cudaStream_t st) {
+    cudaError_t e = run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, st);
+    if (e != cudaSuccess) return e;
+    return dense_sweep<0>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
 }
 
-cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y,
-                        uint32_t nrhs, uint32_t *counters, uint32_t *ticket, uint32_t *status,
-                        cudaStream_t st) {
-    cudaError_t e = dense_sweep<1>(S, val, y, P.n, nrhs, counters, ticket, status, st);
-    if (e != cudaSuccess) return e;
-    if (S.t > 0) {
-        if ((e = reset(counters, P.n, ticket, st)) != cudaSuccess) return e;
-        k_sparse_upper<<<warp_blocks(P.n), 256, 0, st>>>(P, S.t, S.doff, val, y, nrhs, S.u_indeg,
-                                                         counters, ticket, status);
-        e = cudaGetLastError();
-    }
+cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val,
+                        const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                        uint32_t *ticket, uint32_t *status, cudaStream_t st) {
+    cudaError_t e = dense_sweep<1>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
+    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, false, st);
+    if (e == cudaSuccess) e = run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, st);
     return e;
 }
 
 cudaError_t solve_upper_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                              float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                              uint32_t *status, cudaStream_t st) {
-    cudaError_t e;
-    if (S.t > 0) {
-        if ((e = reset(counters, P.n, ticket, st)) != cudaSuccess) return e;
-        k_sparse_upper_trans<<<warp_blocks(P.n), 256, 0, st>>>(P, S.t, S.doff, val, y, nrhs,
-                                                               counters, ticket, status);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    return dense_sweep<2>(S, val, y, P.n, nrhs, counters, ticket, status, st);
+                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                              uint32_t *ticket, uint32_t *status, cudaStream_t st) {
+    cudaError_t e = run_sweep<SWEEP_UT>(P, S, val, y, xo, nrhs, st);
+    if (e == cudaSuccess) e = dense_sweep<2>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
+    return e;
 }
 
 cudaError_t solve_lower_unit_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
-                                   float *y, uint32_t nrhs, uint32_t *counters, uint32_t *ticket,
-                                   uint32_t *status, cudaStream_t st) {
-    cudaError_t e = dense_sweep<3>(S, val, y, P.n, nrhs, counters, ticket, status, st);
-    if (e != cudaSuccess) return e;
-    if (S.t > 0) {
-        if ((e = reset(counters, P.n, ticket, st)) != cudaSuccess) return e;
-        k_sparse_lower_trans<<<warp_blocks(S.t), 256, 0, st>>>(P, S.t, val, y, nrhs, counters,
-                                                               ticket, status);
-        e = cudaGetLastError();
-    }
+                                   const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
+                                   uint32_t *ticket, uint32_t *status, cudaStream_t st) {
+    cudaError_t e = dense_sweep<3>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
+    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, true, st);
+    if (e == cudaSuccess) e = run_sweep<SWEEP_LT>(P, S, val, y, xo, nrhs, st);
     return e;
 }
 

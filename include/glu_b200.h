@@ -188,7 +188,10 @@ typedef struct {
     uint32_t chain_cluster;    /* CTAs of the cluster running narrow-level runs  */
     uint32_t group_lanes;      /* lanes per (column, update-target) pair: 4..32  */
     uint32_t dense_tail_min;   /* smallest trailing block factored densely (0=off)*/
-    float dense_tail_density;  /* density that starts the dense trailing block   */
+    uint32_t dense_tail_max;   /* largest trailing block factored in a buffer    */
+    uint32_t solve_thin;       /* solve levels with at most this many columns run
+                                  in the cluster kernel                          */
+    uint32_t solve_cluster;    /* CTAs of that cluster (1..16)                   */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);
