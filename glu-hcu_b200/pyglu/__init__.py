@@ -416,6 +416,20 @@ class BatchedGLU:
         return {k: getattr(st, k) for k, _ in _capi.Stats._fields_}
 
 
+def write_mtx(path, data, indices, indptr, n):
+    """Write a CSC matrix as a Matrix Market 'coordinate real general' file with
+    triplets column by column -- the order lu_cmd's reader requires
+    (src/nicslu/util/nicslu_readfile.c:98-228).  Values round-trip exactly."""
+    data = np.asarray(data, np.float64)
+    rows = np.asarray(indices, np.int64) + 1
+    cols = np.repeat(np.arange(n, dtype=np.int64), np.diff(np.asarray(indptr, np.int64))) + 1
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{n} {n} {data.size}\n")
+        for r, c, v in zip(rows.tolist(), cols.tolist(), data.tolist()):
+            f.write(f"{r} {c} {v!r}\n")
+
+
 def read_mtx(path):
     """Matrix Market file -> (data, indices, indptr, n) with NICSLU's reader."""
     import ctypes as C
