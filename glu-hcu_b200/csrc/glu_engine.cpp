@@ -658,6 +658,42 @@ Status solve_f32(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, 
 
 }  // namespace
 
+namespace glu {
+
+int handle_device(const glu_handle_s *h) { return h->device; }
+
+Status solve_f32_scratch(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, float *x, float *y,
+                         float *xo, uint32_t *flags, uint32_t *ticket, size_t max_values, uint32_t max_blocks,
+                         void *stream) {
+    if (!h->factored) return set_error(GLU_ERR_STATE, "solve before factorization");
+    if (inst >= h->batch) return set_error(GLU_ERR_ARG, "value set %u outside batch", inst);
+    if (nrhs == 0) return GLU_OK;
+    if (!b || !x) return set_error(GLU_ERR_ARG, "null vector");
+    if (size_t(h->n) * nrhs > max_values)
+        return set_error(GLU_ERR_UNSUPPORTED, "n * nrhs = %zu exceeds the %zu values of the static scratch",
+                         size_t(h->n) * nrhs, max_values);
+    const uint32_t blocks = (h->m + 63) / 64;
+    if (blocks + 1 > max_blocks)
+        return set_error(GLU_ERR_UNSUPPORTED, "dense trailing block of order %u exceeds the static scratch", h->m);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
+    const TransformDev &T = h->T;
+    GLU_CUDA(launch_transform_f32(T.in_idx, T.in_scale, b, y, h->n, nrhs, st), "transform");
+    const float *val = h->d_val.as<float>() + size_t(inst) * h->nnz;
+    const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(inst) * h->m * h->m : val;
+    uint32_t *status = h->d_status.as<uint32_t>();
+    GLU_CUDA(solve_lower_unit(h->P, h->S, val, dval, y, xo, nrhs, flags, ticket, status, st), "lower solve");
+    GLU_CUDA(solve_upper(h->P, h->S, val, dval, y, xo, nrhs, flags, ticket, status, st), "upper solve");
+    GLU_CUDA(launch_transform_f32(T.out_idx, T.out_scale, y, x, h->n, nrhs, st), "transform");
+    uint32_t fl = 0;
+    Status s = read_status(h, st, &fl);
+    if (s != GLU_OK) return s;
+    if (fl & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
+    return GLU_OK;
+}
+
+}  // namespace glu
+
 // ===================================================================== C ABI ==
 extern "C" {
 

@@ -33,4 +33,14 @@ void predict_lu(const SymbolicData &s, const double *ax, float *val);
 // CSR transpose with CSC positions, from a CSC pattern alone.
 void build_csr(SymbolicData &s);
 
+// Device of a handle.
+int handle_device(const glu_handle_s *h);
+// FP32 solve of value set inst with device vectors b, x (nrhs x n) whose
+// working vectors come from caller-provided device memory: y and xo hold
+// max_values floats each, flags holds max_blocks words, ticket one word.
+// Allocates nothing.
+Status solve_f32_scratch(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, float *x, float *y,
+                         float *xo, uint32_t *flags, uint32_t *ticket, size_t max_values, uint32_t max_blocks,
+                         void *stream);
+
 }  // namespace glu

@@ -35,7 +35,7 @@ ENGINE_SYMBOLS = [
     "glu_create", "glu_create_from_pattern", "glu_destroy", "glu_levels", "glu_set_transform",
     "glu_set_source", "glu_load_lu_values", "glu_store_lu_values", "glu_load_source_values",
     "glu_factor", "glu_solve", "glu_solve_transposed", "glu_solve_refined", "glu_get_stats",
-    "glu_get_tuning", "glu_set_tuning",
+    "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc",
 ]
 PRE_SYMBOLS = [
     "glu_pre_analyze", "glu_pre_n", "glu_pre_nnz", "glu_pre_matrix", "glu_pre_transform",
@@ -113,6 +113,7 @@ def load_engine():
         "glu_get_stats": [_vp, C.POINTER(Stats)],
         "glu_get_tuning": [_vp, C.POINTER(Tuning)],
         "glu_set_tuning": [_vp, C.POINTER(Tuning)],
+        "glu_solve_noalloc": [_vp, _u32, _u32, _vp, _vp, _vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -145,6 +145,22 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
  * scale b, unit-L sweep, U sweep, permute and scale back.  x may alias b. */
 glu_status glu_solve(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
                      glu_memory where, glu_stream stream);
+/* glu_solve for callers that cannot allocate device memory.  No counterpart in
+ * the reference.  glu_solve allocates its working vectors on first use; some
+ * hosts may not call cudaMalloc while they run (device memory owned and pooled
+ * by a framework, code running during CUDA graph capture, real-time loops that
+ * must not stall in the allocator).  This variant takes the working vectors
+ * from a fixed array of about 8 MiB that the library keeps in the memory of
+ * every GPU that loads it, for the life of the process, and calls no
+ * allocating routine.  b and x are device pointers (nrhs x n FP32), the handle
+ * must be factored.  Limits: n * nrhs <= 1,048,576 and a dense trailing block
+ * of order <= 262,080; larger problems return GLU_ERR_UNSUPPORTED.  The first
+ * call on a device looks up that array's device address (once per device), so
+ * make the first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (other streams, other handles, other
+ * host threads) race and must be serialized by the caller. */
+glu_status glu_solve_noalloc(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
+                             glu_stream stream);
 /* FP32 solve of A^T x = b with the same factors (U^T then L^T sweeps). */
 glu_status glu_solve_transposed(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b,
                                 float *x, glu_memory where, glu_stream stream);
