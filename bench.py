@@ -42,16 +42,19 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="mesh", choices=["mesh", "nodal", "batch"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--reference-gpu", action="store_true",
+                   help="also time the reference's own numeric.cu (LUonDevice) on the same arrays")
+    p.add_argument("--side", type=int, default=700, help="mesh side (workload mesh)")
     return p.parse_args()
 
 
-def workload(name):
+def workload(name, side=700):
     from pyglu import synth
 
     if name == "mesh":
-        A = synth.config1()
+        A = synth.config1(side=side)
         return dict(A=A, batch=1, nrhs=1, tol=1e-12, values=2,
-                    desc="power-grid mesh 700x700, n=490000, 1 RHS, refine to 1e-12",
+                    desc=f"power-grid mesh {side}x{side}, n={side * side}, 1 RHS, refine to 1e-12",
                     b=lambda n, k, s: synth.rhs_loads(n, seed=s)[None, :])
     if name == "nodal":
         A = synth.config0()
@@ -165,7 +168,7 @@ def cpu_reference(W, steps, warmup, sample_only=False):
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
-    W = workload(args.workload)
+    W = workload(args.workload, args.side)
     if args.impl == "reference":
         if rank != 0:
             return
@@ -295,13 +298,47 @@ def main():
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     nnz_lu = an.nnz_lu
-    alg_bytes = (8.0 * B + 8.0) * nnz_lu  # values read+written per set, row + CSR index once
-    achieved = alg_bytes / (factor_ms / 1e3) / 1e9
     flops = st.factor_flops * B
+    # dominant kernel, timed live: one more factorization with CUDA events
+    # around every launch on the factor stream
+    _capi.check(eng.glu_profile_enable(handle, 1))
+    _capi.check(eng.glu_load_source_values(handle, 0, B, _capi.C.c_void_p(d_vals[0].data_ptr()), _capi.GLU_DEVICE, sp_))
+    _capi.check(eng.glu_factor(handle, 0, B, 0, sp_), "factor")
+    torch.cuda.synchronize()
+    kt = _capi.kernel_times(handle)
+    _capi.check(eng.glu_profile_enable(handle, 0))
+    dom = max(kt, key=lambda k: kt[k][0])
+    dom_ms, dom_n = kt[dom]
+    pat = an.pattern()
+    cp, dg = pat["sym_c_ptr"].astype(np.int64), pat["l_col_ptr"].astype(np.int64)
+    rp, rd = pat["csr_r_ptr"].astype(np.int64), pat["csr_diag_ptr"].astype(np.int64)
+    m_t = int(st.dense_tail)
+    t_s = n - m_t
+    Lk, Uk = cp[1:] - dg - 1, rp[1:] - rd - 1
+    steps_k0 = np.arange(0, m_t, 64)
+    mp = np.maximum(m_t - steps_k0 - 64, 0).astype(np.float64)
+    if dom in ("k_factor_level", "k_factor_chain", "k_scale_level"):
+        # one FP32 read-modify-write of the target per update, L(:,k) read per target
+        upd = float((Lk[:t_s] * Uk[:t_s]).sum())
+        dom_bytes = 8.0 * upd * B
+        dom_flops = 2.0 * upd * B
+    elif dom == "k_dense_update":
+        dom_bytes = float((8.0 * mp * mp + 2 * 4.0 * 64 * mp).sum()) * B
+        dom_flops = float((2.0 * 64 * mp * mp).sum()) * B
+    else:  # panel: diagonal block + L21 rows + U12 columns read and written
+        dom_bytes = float((8.0 * (64 * 64 + 2 * 64 * mp)).sum()) * B
+        dom_flops = float((2.0 * 64 * 64 * mp).sum()) * B
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": None, "kernel": "factorization (all kernels of one glu_factor call)",
+            "traffic": None, "kernel": dom, "launches": dom_n, "kernel_ms": dom_ms,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "fp32_tflops": flops / (factor_ms / 1e3) / 1e12}
+            "algorithmic_bytes": dom_bytes,
+            "fp32_tflops": dom_flops / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0,
+            "fp32_peak_tflops_derived": fp32_peak,
+            "factor_breakdown_ms": {k: round(v[0], 4) for k, v in kt.items() if v[1]},
+            "factor_fp32_tflops": flops / (factor_ms / 1e3) / 1e12}
 
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -314,6 +351,30 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": roof, "gpu_launches": int(st.factor_launches) * args.steps, "clocks": clk}
+    if rank == 0 and world == 1 and B == 1 and args.reference_gpu:
+        # the reference's own numeric.cu (LUonDevice) on the same arrays and values
+        try:
+            import oracle
+
+            if oracle.ref_gpu_available():
+                p = an.pattern()
+                lp, li = lu.levels()
+                placed = np.zeros(an.nnz_lu, np.float32)
+                placed[an.src_slot] = (vals[0] * an.src_scale).astype(np.float32)
+                # keep its n-long scratch columns below 2^32 elements (numeric.cu:44,82,99)
+                keep = 0
+                if n * 8000 > (1 << 31):
+                    keep = (4 << 30) + 12 * an.nnz_lu + (64 << 20) + 8000 * 4 * n
+                ref_ms = []
+                t0 = time.perf_counter()
+                _, rms = oracle.ref_luondevice(p, placed, lp, li, keep_free_bytes=keep)
+                ref_ms.append(rms)
+                line["reference_numeric_cu"] = {
+                    "total_gpu_ms": ref_ms[-1], "includes": "its allocations, copies in and out (numeric.cu:431-625)",
+                    "wall_ms": (time.perf_counter() - t0) * 1e3, "ballast_free_bytes": keep,
+                    "ours_refactor_ms": factor_ms}
+        except Exception as e:  # pragma: no cover
+            line["reference_numeric_cu"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             import oracle

@@ -73,7 +73,65 @@ static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
     return cudaMemcpy(d.p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice);
 }
 
+// Kernel kinds of glu_factor for the optional per-kernel profile.
+enum KernelKind {
+    KK_PERT = 0, KK_LEVEL, KK_CHAIN, KK_SCALE, KK_DGATHER, KK_PANEL, KK_UPDATE, KK_DSCATTER, KK_CHECK,
+    KK_SN_PANEL, KK_SN_UPDATE
+};
+static const char *const kKindNames[GLU_KERNEL_KINDS] = {
+    "k_colsum+k_pert_finish", "k_factor_level", "k_factor_chain", "k_scale_level", "k_dense_gather",
+    "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_panel", "k_sn_update"};
+
+// Events around every launch of one glu_factor call, when enabled.
+struct KernelProfiler {
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;
+    size_t used = 0;
+    float ms[GLU_KERNEL_KINDS] = {};
+    uint32_t n[GLU_KERNEL_KINDS] = {};
+    cudaError_t begin(cudaStream_t st) {
+        if (!on) return cudaSuccess;
+        while (ev.size() < 2 * (used + 1)) {
+            cudaEvent_t e;
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return r;
+            ev.push_back(e);
+        }
+        return cudaEventRecord(ev[2 * used], st);
+    }
+    cudaError_t end(int k, cudaStream_t st) {
+        if (!on) return cudaSuccess;
+        if (kind.size() < used + 1) kind.resize(used + 1);
+        kind[used] = k;
+        cudaError_t r = cudaEventRecord(ev[2 * used + 1], st);
+        ++used;
+        return r;
+    }
+    void collect() {
+        if (!on) return;
+        for (int k = 0; k < GLU_KERNEL_KINDS; ++k) {
+            ms[k] = 0;
+            n[k] = 0;
+        }
+        for (size_t i = 0; i < used; ++i) {
+            float t = 0;
+            cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]);
+            ms[kind[i]] += t;
+            n[kind[i]]++;
+        }
+        used = 0;
+    }
+    ~KernelProfiler() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
+
 enum StepKind { STEP_LEVEL = 0, STEP_CHAIN = 1 };
+// One level of the supernodal schedule: supernodes [i0, i1) of the level order.
+struct SnLevel {
+    uint32_t i0, i1, pblocks, ublocks, atomic;
+};
 struct Step {
     int kind;
     uint32_t l0, l1;  // sparse levels [l0, l1)
@@ -110,6 +168,13 @@ struct glu_handle_s {
     uint32_t chain_cluster = 8;
     FactorPlanDev F{};
     double flops = 0;
+    // supernodal plan of the sparse part (used when tune.sn_width != 0)
+    bool use_sn = false;
+    uint32_t nsn = 0;
+    DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_dscr, d_sn_scratch;
+    std::vector<SnLevel> sn_levels;
+    uint64_t sn_scr_stride = 0;
+    SnPlanDev SN{};
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
     std::vector<SweepStep> sw_steps[4];
@@ -130,6 +195,7 @@ struct glu_handle_s {
     double *h_norms = nullptr;     // pinned
     size_t h_norms_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    KernelProfiler prof;
     bool factored = false;
     glu_stats stats{};
 
@@ -319,6 +385,113 @@ uint32_t pick_group(double avg_l, uint32_t forced) {
     return 32;
 }
 
+// Supernodal schedule of the sparse columns [0, t).  Column k joins the
+// supernode [s0, k) when k - s0 < width, Lpat(k-1) = {k} u Lpat(k), and the
+// rows s0..k-1 of column k are all present (dense diagonal block).  A
+// supernode's level is one more than the largest level among the supernodes
+// holding its columns' dependencies (symbolic.cc:106-151: U(c',c) != 0 with
+// Lpat(c') nonempty, and L(c,c') != 0).
+Status build_sn_plan(glu_handle_s *h) {
+    const SymbolicData &s = h->pat;
+    const uint32_t t = h->t;
+    const uint32_t width = std::min<uint32_t>(h->tune.sn_width, kSnMaxWidth);
+    h->use_sn = width > 0 && t > 0;
+    h->nsn = 0;
+    h->sn_levels.clear();
+    if (!h->use_sn) return GLU_OK;
+    auto nl = [&](uint32_t c) { return s.sym_c_ptr[c + 1] - s.l_col_ptr[c] - 1; };
+    auto nu = [&](uint32_t c) { return s.csr_r_ptr[c + 1] - s.csr_diag_ptr[c] - 1; };
+    std::vector<uint32_t> first(1, 0);
+    for (uint32_t k = 1, s0 = 0; k < t; ++k) {
+        bool join = k - s0 < width && nl(k - 1) == nl(k) + 1 && s.sym_r_idx[s.l_col_ptr[k - 1] + 1] == k &&
+                    s.l_col_ptr[k] >= s.sym_c_ptr[k] + (k - s0) && s.sym_r_idx[s.l_col_ptr[k] - (k - s0)] == s0;
+        if (join)
+            join = std::equal(s.sym_r_idx.begin() + s.l_col_ptr[k - 1] + 2, s.sym_r_idx.begin() + s.sym_c_ptr[k],
+                              s.sym_r_idx.begin() + s.l_col_ptr[k] + 1);
+        if (!join) {
+            first.push_back(k);
+            s0 = k;
+        }
+    }
+    const uint32_t ns = uint32_t(first.size());
+    first.push_back(t);
+    std::vector<uint32_t> sn_of(t);
+    for (uint32_t q = 0; q < ns; ++q)
+        for (uint32_t c = first[q]; c < first[q + 1]; ++c) sn_of[c] = q;
+    std::vector<int32_t> lev(ns, 0);
+    int32_t nlev = 0;
+    for (uint32_t q = 0; q < ns; ++q) {
+        const uint32_t s0 = first[q];
+        int32_t mx = -1;
+        for (uint32_t c = s0; c < first[q + 1]; ++c) {
+            for (uint32_t p = s.sym_c_ptr[c]; p < s.l_col_ptr[c]; ++p) {
+                const uint32_t r = s.sym_r_idx[p];
+                if (r < s0 && nl(r) > 0) mx = std::max(mx, lev[sn_of[r]]);
+            }
+            for (uint32_t e = s.csr_r_ptr[c]; e < s.csr_diag_ptr[c]; ++e) {
+                const uint32_t c2 = s.csr_c_idx[e];
+                if (c2 < s0) mx = std::max(mx, lev[sn_of[c2]]);
+            }
+        }
+        lev[q] = mx + 1;
+        nlev = std::max(nlev, mx + 2);
+    }
+    // level order (ascending column within a level)
+    std::vector<uint32_t> lcount(size_t(nlev) + 1, 0);
+    for (uint32_t q = 0; q < ns; ++q) lcount[lev[q] + 1]++;
+    for (int32_t l = 0; l < nlev; ++l) lcount[l + 1] += lcount[l];
+    std::vector<uint32_t> order(ns);
+    {
+        std::vector<uint32_t> cur(lcount.begin(), lcount.end() - 1);
+        for (uint32_t q = 0; q < ns; ++q) order[cur[lev[q]]++] = q;
+    }
+    std::vector<uint32_t> col(ns), wid(ns), pblk(size_t(ns) + 1, 0), ublk(size_t(ns) + 1, 0), dscr(ns, 0);
+    uint64_t scr_max = 0;
+    const uint32_t PT = kSnPanelThreads, UT = 64;
+    for (int32_t l = 0; l < nlev; ++l) {
+        uint64_t scr = 0;
+        uint32_t updating = 0;
+        for (uint32_t i = lcount[l]; i < lcount[l + 1]; ++i) {
+            const uint32_t q = order[i];
+            const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
+            const uint64_t m = nl(last), nt = nu(last);
+            col[i] = first[q];
+            wid[i] = w;
+            uint64_t pb, ub;
+            const uint64_t tiles = ((m + UT - 1) / UT) * ((nt + UT - 1) / UT);
+            if (w == 1) {
+                pb = (m + PT - 1) / PT;
+                ub = tiles;
+            } else {
+                pb = 1 + (m + PT - 1) / PT + (nt + PT - 1) / PT;
+                ub = 1 + tiles;
+                dscr[i] = uint32_t(scr);
+                scr += uint64_t(w) * w;
+            }
+            if (tiles) ++updating;
+            if (uint64_t(pblk[i]) + pb > UINT32_MAX || uint64_t(ublk[i]) + ub > UINT32_MAX)
+                return set_error(GLU_ERR_UNSUPPORTED, "supernodal schedule too large");
+            pblk[i + 1] = pblk[i] + uint32_t(pb);
+            ublk[i + 1] = ublk[i] + uint32_t(ub);
+        }
+        scr_max = std::max(scr_max, scr);
+        const uint32_t i0 = lcount[l], i1 = lcount[l + 1];
+        h->sn_levels.push_back(SnLevel{i0, i1, pblk[i1] - pblk[i0], ublk[i1] - ublk[i0], updating > 1 ? 1u : 0u});
+    }
+    h->nsn = ns;
+    h->sn_scr_stride = std::max<uint64_t>(scr_max, 1);
+    GLU_CUDA(upload(h->d_sn_col, col), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_w, wid), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_pblk, pblk), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_ublk, ublk), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_dscr, dscr), "upload supernodes");
+    h->d_sn_scratch.release();
+    GLU_CUDA(h->d_sn_scratch.alloc(sizeof(float) * h->sn_scr_stride * h->batch), "allocate supernode scratch");
+    h->SN = SnPlanDev{h->d_sn_col.as<uint32_t>(), h->d_sn_w.as<uint32_t>(), h->d_sn_pblk.as<uint32_t>(),
+                      h->d_sn_ublk.as<uint32_t>(), h->d_sn_dscr.as<uint32_t>()};
+    return GLU_OK;
+}
+
 Status build_plan(glu_handle_s *h) {
     const SymbolicData &s = h->pat;
     const uint32_t n = h->n;
@@ -469,14 +642,23 @@ Status build_plan(glu_handle_s *h) {
         sp.nlev = uint32_t(lptr.size() - 1);
     }
 
+    Status sn = build_sn_plan(h);
+    if (sn != GLU_OK) return sn;
     uint32_t wide = 0, chains = 0;
     for (auto &st : h->steps) (st.kind == STEP_CHAIN ? chains : wide)++;
-    h->stats.wide_levels = wide;
-    h->stats.chain_segments = chains;
+    h->stats.wide_levels = h->use_sn ? 0 : wide;
+    h->stats.chain_segments = h->use_sn ? 0 : chains;
     h->stats.dense_tail = m;
     h->stats.factor_flops = flops;
-    uint64_t launches = h->steps.size() + (NL ? 1 : 0) + 2;
-    if (m) launches += 2 * ((m + kDenseNB - 1) / kDenseNB);
+    h->stats.supernodes = h->nsn;
+    h->stats.sn_levels = uint32_t(h->sn_levels.size());
+    uint64_t launches = 2;
+    if (h->use_sn) {
+        for (const SnLevel &lv : h->sn_levels) launches += (lv.pblocks ? 1 : 0) + (lv.ublocks ? 1 : 0);
+    } else {
+        launches += h->steps.size() + (NL ? 1 : 0);
+    }
+    if (m) launches += 2 * ((m + kDenseNB - 1) / kDenseNB) + (h->dense_buffer ? 2 : 0);
     h->stats.factor_launches = launches;
     return GLU_OK;
 }
@@ -508,7 +690,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 16384u, 128u, 4u};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 16384u, 128u, 4u, kSnMaxWidth};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -964,46 +1146,81 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     const float *pert = nullptr;
     GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
     GLU_CUDA(cudaEventRecord(h->ev0, st), "event");
+    KernelProfiler &pf = h->prof;
+    pf.used = 0;
+#define GLU_LAUNCH(kind, call, what)                    \
+    do {                                                \
+        GLU_CUDA(pf.begin(st), "profile event");        \
+        GLU_CUDA((call), (what));                       \
+        GLU_CUDA(pf.end((kind), st), "profile event");  \
+    } while (0)
     if (perturb) {
-        GLU_CUDA(launch_pert(h->P, val, stride, count, h->d_colmax.as<float>(),
-                             h->d_pert.as<float>() + first, st), "perturbation");
+        GLU_LAUNCH(KK_PERT, launch_pert(h->P, val, stride, count, h->d_colmax.as<float>(), h->d_pert.as<float>() + first, st),
+                   "perturbation");
         pert = h->d_pert.as<float>() + first;
     }
-    const uint32_t NL = uint32_t(h->levels_h.size());
-    for (const Step &stp : h->steps) {
+    const uint32_t NL = h->use_sn ? 0u : uint32_t(h->levels_h.size());
+    if (h->use_sn) {
+        float *scr = h->d_sn_scratch.as<float>() + size_t(first) * h->sn_scr_stride;
+        for (const SnLevel &lv : h->sn_levels) {
+            if (lv.pblocks)
+                GLU_LAUNCH(KK_SN_PANEL,
+                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, scr, h->sn_scr_stride, lv.i0,
+                                           lv.i1, lv.pblocks, st),
+                           "factor (supernode panels)");
+            if (lv.ublocks)
+                GLU_LAUNCH(KK_SN_UPDATE,
+                           launch_sn_update(h->P, h->SN, val, stride, count, scr, h->sn_scr_stride, lv.i0, lv.i1,
+                                            lv.ublocks, lv.atomic, st),
+                           "factor (supernode updates)");
+        }
+    }
+    for (const Step &stp : (h->use_sn ? std::vector<Step>() : h->steps)) {
         if (stp.kind == STEP_CHAIN) {
-            GLU_CUDA(launch_factor_chain(h->P, h->F, val, stride, count, pert, stp.l0, stp.l1, h->chain_cluster, st),
-                     "factor (narrow levels)");
+            GLU_LAUNCH(KK_CHAIN,
+                       launch_factor_chain(h->P, h->F, val, stride, count, pert, stp.l0, stp.l1, h->chain_cluster, st),
+                       "factor (narrow levels)");
         } else {
             const LevelInfo &cur = h->levels_h[stp.l0];
             const LevelInfo *prev = stp.l0 > 0 ? &h->levels_h[stp.l0 - 1] : nullptr;
-            GLU_CUDA(launch_factor_level(h->P, h->F, val, stride, count, pert, cur, prev, h->items_h[stp.l0], st),
-                     "factor (level)");
+            GLU_LAUNCH(KK_LEVEL,
+                       launch_factor_level(h->P, h->F, val, stride, count, pert, cur, prev, h->items_h[stp.l0], st),
+                       "factor (level)");
         }
     }
-    if (NL) GLU_CUDA(launch_scale_level(h->P, h->F, val, stride, count, pert, h->levels_h[NL - 1], st), "factor (scale)");
+    if (NL)
+        GLU_LAUNCH(KK_SCALE, launch_scale_level(h->P, h->F, val, stride, count, pert, h->levels_h[NL - 1], st),
+                   "factor (scale)");
     // dense trailing block: in place, or through the dense buffer
     float *dbase = h->dense_buffer ? h->d_dense.as<float>() + size_t(first) * h->m * h->m : val;
     const uint64_t dstride = h->dense_buffer ? uint64_t(h->m) * h->m : stride;
     if (h->m && h->dense_buffer)
-        GLU_CUDA(launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
-                 "factor (dense gather)");
+        GLU_LAUNCH(KK_DGATHER,
+                   launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
+                   "factor (dense gather)");
     for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
         uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
         uint32_t last_has_l = 0;  // the last column of the matrix has no L part
-        GLU_CUDA(launch_dense_panel(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
-                                    h->d_diag_scratch.as<float>(), last_has_l, st), "factor (dense panel)");
-        GLU_CUDA(launch_dense_update(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
-                                     h->d_diag_scratch.as<float>(), st), "factor (dense update)");
+        GLU_LAUNCH(KK_PANEL,
+                   launch_dense_panel(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
+                                      h->d_diag_scratch.as<float>(), last_has_l, st),
+                   "factor (dense panel)");
+        GLU_LAUNCH(KK_UPDATE,
+                   launch_dense_update(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
+                                       h->d_diag_scratch.as<float>(), st),
+                   "factor (dense update)");
     }
     if (h->m && h->dense_buffer)
-        GLU_CUDA(launch_dense_scatter(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
-                 "factor (dense scatter)");
-    GLU_CUDA(launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
+        GLU_LAUNCH(KK_DSCATTER,
+                   launch_dense_scatter(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
+                   "factor (dense scatter)");
+    GLU_LAUNCH(KK_CHECK, launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
+#undef GLU_LAUNCH
     GLU_CUDA(cudaEventRecord(h->ev1, st), "event");
     uint32_t flags = 0;
     s = read_status(h, st, &flags);
     if (s != GLU_OK) return s;
+    pf.collect();
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.last_factor_ms = ms;
@@ -1131,6 +1348,26 @@ glu_status glu_get_stats(glu_handle_t h, glu_stats *stats) {
     if (!h || !stats) return set_error(GLU_ERR_ARG, "null argument");
     *stats = h->stats;
     return GLU_OK;
+}
+
+glu_status glu_profile_enable(glu_handle_t h, int on) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    h->prof.on = on != 0;
+    h->prof.used = 0;
+    return GLU_OK;
+}
+
+glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    for (int k = 0; k < GLU_KERNEL_KINDS; ++k) {
+        if (ms) ms[k] = h->prof.ms[k];
+        if (launches) launches[k] = h->prof.n[k];
+    }
+    return GLU_OK;
+}
+
+const char *glu_kernel_kind_name(int kind) {
+    return (kind >= 0 && kind < GLU_KERNEL_KINDS) ? kKindNames[kind] : "";
 }
 
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t) {

@@ -229,26 +229,34 @@ __global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uin
     }
 }
 
-// Trailing update A22 -= L21 U12 on a 128 x 128 tile per block (256 threads,
-// 8 x 8 outputs each, K = kb <= 64 staged once in shared memory).  Block (0,0)
-// first writes the factored diagonal block back from diag_scratch.
-constexpr int kTB = kGemmTile;
-constexpr int kLDB = kTB + 4;
-constexpr int kLDC = kTB + 1;
-constexpr size_t kUpdateSmem =
-    (size_t(kDenseNB) * kTB + size_t(kDenseNB) * kLDB) * 4 > size_t(kTB) * kLDC * 4
-        ? (size_t(kDenseNB) * kTB + size_t(kDenseNB) * kLDB) * 4
-        : size_t(kTB) * kLDC * 4;
+// Trailing update A22 -= L21 U12 on a TB x TB tile per block (256 threads as a
+// 16 x 16 grid, RM x RM outputs each, K = kb <= 64 staged once in shared
+// memory).  TB = 128 for large trailing blocks, 64 when 128-wide tiles would
+// leave SMs idle.  Block (0,0) first writes the factored diagonal block back
+// from diag_scratch.
+template <int TB>
+struct UpdateTile {
+    static constexpr int RM = TB / 16;
+    static constexpr int LDB = TB + 4;
+    static constexpr int LDC = TB + 1;
+    static constexpr size_t AB = (size_t(kDenseNB) * TB + size_t(kDenseNB) * LDB) * 4;
+    static constexpr size_t C = size_t(TB) * LDC * 4;
+    static constexpr size_t Smem = AB > C ? AB : C;
+};
 
+template <int TB>
 __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64_t stride,
                                                          const uint32_t *__restrict__ doff,
                                                          uint32_t m, uint32_t k0, uint32_t kb,
                                                          const float *diag_scratch) {
+    constexpr int RM = UpdateTile<TB>::RM;
+    constexpr int LDB = UpdateTile<TB>::LDB;
+    constexpr int LDC = UpdateTile<TB>::LDC;
     extern __shared__ float4 smem4[];
     float *smem = reinterpret_cast<float *>(smem4);
-    float *sA = smem;                       // [k][row]
-    float *sB = smem + kDenseNB * kTB;      // [k][col], padded
-    float *sC = smem;                       // [col][row], padded (reuses sA/sB)
+    float *sA = smem;                    // [k][row]
+    float *sB = smem + kDenseNB * TB;    // [k][col], padded
+    float *sC = smem;                    // [col][row], padded (reuses sA/sB)
     float *val = val_base + blockIdx.z * stride;
     const uint32_t tid = threadIdx.x;
     if (blockIdx.x == 0 && blockIdx.y == 0) {
@@ -261,73 +269,76 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     const uint32_t r0 = k0 + kb;
     if (r0 >= m) return;
     const uint32_t mp = m - r0;
-    const uint32_t rbase = blockIdx.x * kTB, cbase = blockIdx.y * kTB;
+    const uint32_t rbase = blockIdx.x * TB, cbase = blockIdx.y * TB;
     if (rbase >= mp || cbase >= mp) return;
     const uint32_t tx = tid & 15, ty = tid >> 4;
     // C tile into registers (through shared memory for coalescing): every
     // entry then receives its updates one k at a time, in increasing k, as in
     // the column algorithm.  (Loops unrolled so that many loads are in flight.)
 #pragma unroll 16
-    for (uint32_t e = tid; e < uint32_t(kTB) * kTB; e += 256) {
-        uint32_t col = e / kTB, row = e - col * kTB;
+    for (uint32_t e = tid; e < uint32_t(TB) * TB; e += 256) {
+        uint32_t col = e / TB, row = e - col * TB;
         float v = 0.0f;
         if (cbase + col < mp && rbase + row < mp) v = ld_cg(val + doff[r0 + cbase + col] + r0 + rbase + row);
-        sC[col * kLDC + row] = v;
+        sC[col * LDC + row] = v;
     }
     __syncthreads();
-    float acc[8][8];
+    float acc[RM][RM];
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < RM; ++j)
 #pragma unroll
-        for (int i = 0; i < 8; ++i) acc[i][j] = sC[(tx * 8 + j) * kLDC + ty * 8 + i];
+        for (int i = 0; i < RM; ++i) acc[i][j] = sC[(tx * RM + j) * LDC + ty * RM + i];
     __syncthreads();
     // stage L21 tile: sA[k][row]
 #pragma unroll 16
-    for (uint32_t e = tid; e < uint32_t(kDenseNB) * kTB; e += 256) {
-        uint32_t k = e / kTB, row = e - k * kTB;
+    for (uint32_t e = tid; e < uint32_t(kDenseNB) * TB; e += 256) {
+        uint32_t k = e / TB, row = e - k * TB;
         float v = 0.0f;
         if (k < kb && rbase + row < mp) v = ld_cg(val + doff[k0 + k] + r0 + rbase + row);
-        sA[k * kTB + row] = v;
+        sA[k * TB + row] = v;
     }
     // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
     {
         uint32_t lane = tid & 31, w = tid >> 5;
 #pragma unroll 8
-        for (uint32_t col = w; col < uint32_t(kTB); col += 8) {
+        for (uint32_t col = w; col < uint32_t(TB); col += 8) {
             bool cok = cbase + col < mp;
             const float *src = cok ? val + doff[r0 + cbase + col] + k0 : nullptr;
 #pragma unroll
             for (uint32_t h = 0; h < uint32_t(kDenseNB); h += 32) {
                 uint32_t k = h + lane;
                 float v = (cok && k < kb) ? ld_cg(src + k) : 0.0f;
-                sB[k * kLDB + col] = v;
+                sB[k * LDB + col] = v;
             }
         }
     }
     __syncthreads();
 #pragma unroll 4
     for (uint32_t k = 0; k < kb; ++k) {
-        float4 a0 = *reinterpret_cast<const float4 *>(sA + k * kTB + ty * 8);
-        float4 a1 = *reinterpret_cast<const float4 *>(sA + k * kTB + ty * 8 + 4);
-        float4 b0 = *reinterpret_cast<const float4 *>(sB + k * kLDB + tx * 8);
-        float4 b1 = *reinterpret_cast<const float4 *>(sB + k * kLDB + tx * 8 + 4);
-        float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-        float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        float av[RM], bv[RM];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int q = 0; q < RM; q += 4) {
+            float4 a4 = *reinterpret_cast<const float4 *>(sA + k * TB + ty * RM + q);
+            float4 b4 = *reinterpret_cast<const float4 *>(sB + k * LDB + tx * RM + q);
+            av[q] = a4.x; av[q + 1] = a4.y; av[q + 2] = a4.z; av[q + 3] = a4.w;
+            bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
+        }
 #pragma unroll
-            for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(-av[i], bv[j], acc[i][j]);
+        for (int i = 0; i < RM; ++i)
+#pragma unroll
+            for (int j = 0; j < RM; ++j) acc[i][j] = fmaf(-av[i], bv[j], acc[i][j]);
     }
     __syncthreads();
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
+    for (int j = 0; j < RM; ++j)
 #pragma unroll
-        for (int i = 0; i < 8; ++i) sC[(tx * 8 + j) * kLDC + ty * 8 + i] = acc[i][j];
+        for (int i = 0; i < RM; ++i) sC[(tx * RM + j) * LDC + ty * RM + i] = acc[i][j];
     __syncthreads();
-    for (uint32_t e = tid; e < uint32_t(kTB) * kTB; e += 256) {
-        uint32_t col = e / kTB, row = e - col * kTB;
+#pragma unroll 4
+    for (uint32_t e = tid; e < uint32_t(TB) * TB; e += 256) {
+        uint32_t col = e / TB, row = e - col * TB;
         if (cbase + col < mp && rbase + row < mp)
-            st_cg(val + doff[r0 + cbase + col] + r0 + rbase + row, sC[col * kLDC + row]);
+            st_cg(val + doff[r0 + cbase + col] + r0 + rbase + row, sC[col * LDC + row]);
     }
 }
 
@@ -358,16 +369,25 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
                                 cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_dense_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(kUpdateSmem));
+        cudaError_t e = cudaFuncSetAttribute(k_dense_update<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(UpdateTile<128>::Smem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_dense_update<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(UpdateTile<64>::Smem));
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    uint32_t rest = m - (k0 + kb);
-    uint32_t tiles = (rest + kTB - 1) / kTB;
-    if (tiles == 0) tiles = 1;
-    dim3 grid(tiles, tiles, count);
-    k_dense_update<<<grid, 256, kUpdateSmem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    const uint32_t rest = m - (k0 + kb);
+    const uint32_t t128 = (rest + 127) / 128;
+    if (uint64_t(t128) * t128 * count >= 2 * 148) {
+        dim3 grid(t128, t128, count);
+        k_dense_update<128><<<grid, 256, UpdateTile<128>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    } else {
+        uint32_t t64 = (rest + 63) / 64;
+        if (t64 == 0) t64 = 1;
+        dim3 grid(t64, t64, count);
+        k_dense_update<64><<<grid, 256, UpdateTile<64>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    }
     return cudaGetLastError();
 }
 

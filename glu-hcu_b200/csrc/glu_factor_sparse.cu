@@ -94,10 +94,11 @@ __device__ __forceinline__ void level_items(const DevPattern &P, const FactorPla
         uint32_t nch = (nl + CH - 1) / CH;
         uint32_t jj = rem / nch, ch = rem - jj * nch;
         uint32_t e0 = ch * CH, e1 = min(e0 + CH, nl);
-        if (atomic)
+        if (atomic) {
             update_item<true>(P, val, k, jj, e0, e1, pert, lane, G);
-        else
+        } else {
             update_item<false>(P, val, k, jj, e0, e1, pert, lane, G);
+        }
     }
 }
 

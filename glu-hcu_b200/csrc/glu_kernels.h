@@ -38,6 +38,30 @@ cudaError_t launch_factor_chain(const DevPattern &P, const FactorPlanDev &F, flo
                                 uint64_t stride, uint32_t count, const float *pert_z, uint32_t l0,
                                 uint32_t l1, uint32_t cluster, cudaStream_t st);
 
+// ------------------------------------------------------- supernodal factor --
+constexpr uint32_t kSnMaxWidth = 64;       // widest supernode
+constexpr uint32_t kSnPanelThreads = 128;  // threads of a panel block (rows or targets per block)
+
+// Supernodes in level order: first column, width; block prefixes of the panel
+// and update launches; offset of the factored diagonal block in the level's
+// scratch.
+struct SnPlanDev {
+    const uint32_t *sn_col;
+    const uint32_t *sn_w;
+    const uint32_t *pblk;  // [count + 1]
+    const uint32_t *ublk;  // [count + 1]
+    const uint32_t *dscr;
+};
+
+// Supernodes [i0, i1) of one level; blocks = pblk[i1] - pblk[i0] (panel) or
+// ublk[i1] - ublk[i0] (update).  scratch: scr_stride floats per value set.
+cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
+                            const float *pert_z, float *scratch, uint64_t scr_stride, uint32_t i0, uint32_t i1,
+                            uint32_t blocks, cudaStream_t st);
+cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
+                             const float *scratch, uint64_t scr_stride, uint32_t i0, uint32_t i1, uint32_t blocks,
+                             uint32_t atomic, cudaStream_t st);
+
 // ------------------------------------------------------------- dense tail --
 // The trailing m x m block [t, n) x [t, n) is fully dense; element (i, j) of it
 // is val[doff[j] + i] (column-major, one base offset per column).

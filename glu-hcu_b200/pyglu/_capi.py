@@ -35,8 +35,10 @@ ENGINE_SYMBOLS = [
     "glu_create", "glu_create_from_pattern", "glu_destroy", "glu_levels", "glu_set_transform",
     "glu_set_source", "glu_load_lu_values", "glu_store_lu_values", "glu_load_source_values",
     "glu_factor", "glu_solve", "glu_solve_transposed", "glu_solve_refined", "glu_get_stats",
-    "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc",
+    "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
+    "glu_kernel_kind_name",
 ]
+GLU_KERNEL_KINDS = 11
 PRE_SYMBOLS = [
     "glu_pre_analyze", "glu_pre_n", "glu_pre_nnz", "glu_pre_matrix", "glu_pre_transform",
     "glu_pre_source_map", "glu_pre_destroy", "glu_pre_read_mtx", "glu_pre_free",
@@ -67,13 +69,14 @@ class Stats(C.Structure):
     _fields_ = [("n", C.c_uint32), ("nnz_lu", C.c_uint32), ("batch", C.c_uint32), ("num_lev", C.c_int32),
                 ("wide_levels", C.c_uint32), ("chain_segments", C.c_uint32), ("dense_tail", C.c_uint32),
                 ("factor_flops", C.c_double), ("factor_launches", C.c_uint64),
-                ("last_factor_ms", C.c_float), ("pert", C.c_float)]
+                ("last_factor_ms", C.c_float), ("pert", C.c_float), ("supernodes", C.c_uint32),
+                ("sn_levels", C.c_uint32)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("wide_work", C.c_uint32), ("chain_cluster", C.c_uint32), ("group_lanes", C.c_uint32),
                 ("dense_tail_min", C.c_uint32), ("dense_tail_max", C.c_uint32), ("solve_thin", C.c_uint32),
-                ("solve_cluster", C.c_uint32)]
+                ("solve_cluster", C.c_uint32), ("sn_width", C.c_uint32)]
 
 
 _vp = C.c_void_p
@@ -114,6 +117,8 @@ def load_engine():
         "glu_get_tuning": [_vp, C.POINTER(Tuning)],
         "glu_set_tuning": [_vp, C.POINTER(Tuning)],
         "glu_solve_noalloc": [_vp, _u32, _u32, _vp, _vp, _vp],
+        "glu_profile_enable": [_vp, C.c_int],
+        "glu_kernel_times": [_vp, _vp, _vp],
     }
     for name, args in sig.items():
         f = getattr(lib, name)
@@ -123,7 +128,18 @@ def load_engine():
     lib.glu_symbolic_destroy.restype = None
     lib.glu_destroy.argtypes = [_vp]
     lib.glu_destroy.restype = None
+    lib.glu_kernel_kind_name.argtypes = [C.c_int]
+    lib.glu_kernel_kind_name.restype = C.c_char_p
     return lib
+
+
+def kernel_times(handle):
+    """{kernel kind: (ms, launches)} of the last profiled glu_factor call."""
+    lib = engine()
+    ms = np.zeros(GLU_KERNEL_KINDS, np.float32)
+    n = np.zeros(GLU_KERNEL_KINDS, np.uint32)
+    check(lib.glu_kernel_times(handle, ptr(ms), ptr(n)), "kernel times")
+    return {lib.glu_kernel_kind_name(k).decode(): (float(ms[k]), int(n[k])) for k in range(GLU_KERNEL_KINDS)}
 
 
 def load_preprocess():

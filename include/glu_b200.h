@@ -195,19 +195,34 @@ typedef struct {
     uint64_t factor_launches;  /* kernel launches of one glu_factor call          */
     float last_factor_ms;      /* device time of the last glu_factor call         */
     float pert;                /* perturbation of the last GESP factorization     */
+    uint32_t supernodes;       /* supernodes of the sparse part (0: column path)   */
+    uint32_t sn_levels;        /* levels of the supernodal schedule               */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
+
+/* Per-kernel device times of glu_factor, for profiling.  After
+ * glu_profile_enable(h, 1) every later glu_factor brackets each launch with
+ * CUDA events on its stream; glu_kernel_times returns, per kernel kind, the
+ * summed milliseconds and launch counts of the last glu_factor call (arrays
+ * of GLU_KERNEL_KINDS entries; see glu_kernel_kind_name).  Off by default:
+ * the events add a little time between launches. */
+#define GLU_KERNEL_KINDS 11
+glu_status glu_profile_enable(glu_handle_t h, int on);
+glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
+const char *glu_kernel_kind_name(int kind);
 
 /* Schedule knobs (the autotuner's search space).  Applies to later calls. */
 typedef struct {
     uint32_t wide_work;        /* a level with more update work runs alone       */
     uint32_t chain_cluster;    /* CTAs of the cluster running narrow-level runs  */
     uint32_t group_lanes;      /* lanes per (column, update-target) pair: 4..32  */
-    uint32_t dense_tail_min;   /* smallest trailing block factored densely (0=off)*/
+    uint32_t dense_tail_min;   /* smallest dense trailing block (above n: none)  */
     uint32_t dense_tail_max;   /* largest trailing block factored in a buffer    */
     uint32_t solve_thin;       /* solve levels with at most this many columns run
                                   in the cluster kernel                          */
     uint32_t solve_cluster;    /* CTAs of that cluster (1..16)                   */
+    uint32_t sn_width;         /* widest supernode of the sparse factorization
+                                  (1..64); 0 factors column by column            */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

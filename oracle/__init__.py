@@ -290,3 +290,60 @@ def fill_in(ap, ai, n, cap=50_000_000):
     if nz == 0:
         raise MemoryError("fill-in exceeds the oracle's capacity")
     return cp, ri[:nz].copy(), dg
+
+
+# ---------------------------------------------------------------------------
+# The reference's own GPU numeric factorization (src/numeric.cu LUonDevice),
+# built for sm_100a into oracle/_ref/libglu_ref_gpu.so.
+_refgpu = None
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libglu_ref_gpu.so"))
+
+
+def _load_ref_gpu():
+    global _refgpu
+    if _refgpu is None:
+        ref = _load_ref()
+        ref.ref_load_pattern.argtypes = [C.c_void_p, C.c_uint, C.c_uint, _u32p, _u32p, _u32p, _u32p, _u32p, _u32p,
+                                         _f32p, C.c_int, _i32p, _i32p]
+        lib = C.CDLL(os.path.join(HERE, "_ref", "libglu_ref_gpu.so"))
+        lib.ref_gpu_luondevice.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_float), C.c_char_p,
+                                           C.c_int]
+        lib.ref_gpu_luondevice.restype = C.c_int
+        _refgpu = lib
+    return _refgpu
+
+
+def ref_luondevice(pattern, val, level_ptr, level_idx, perturb=False, keep_free_bytes=0):
+    """Run the reference's LUonDevice on the given Symbolic_Matrix arrays.
+
+    Returns (factor values, the reference's own "Total GPU time" in ms, which
+    includes its allocations and copies).  keep_free_bytes > 0 holds a ballast
+    allocation so that only that much device memory is free during the call
+    (bounds the scratch the reference sizes from free memory).
+    """
+    lib = _load_ref_gpu()
+    ref = _load_ref()
+    h = ref.ref_create()
+    try:
+        p = {k: np.ascontiguousarray(pattern[k], np.uint32) for k in
+             ("sym_c_ptr", "sym_r_idx", "l_col_ptr", "csr_r_ptr", "csr_c_idx", "csr_diag_ptr")}
+        n = p["sym_c_ptr"].size - 1
+        nnz = p["sym_r_idx"].size
+        lp = np.ascontiguousarray(level_ptr, np.int32)
+        li = np.ascontiguousarray(level_idx, np.int32)
+        ref.ref_load_pattern(h, n, nnz, p["sym_c_ptr"], p["sym_r_idx"], p["l_col_ptr"], p["csr_r_ptr"],
+                             p["csr_c_idx"], p["csr_diag_ptr"], np.ascontiguousarray(val, np.float32),
+                             lp.size - 1, lp, li)
+        ms = C.c_float(0)
+        err = C.create_string_buffer(1024)
+        st = lib.ref_gpu_luondevice(h, int(perturb), int(keep_free_bytes), C.byref(ms), err, 1024)
+        if st != 0:
+            raise RuntimeError(f"reference LUonDevice failed: {err.value.decode(errors='replace')}")
+        out = np.empty(nnz, np.float32)
+        ref.ref_get_val(h, out)
+        return out, float(ms.value)
+    finally:
+        ref.ref_destroy(h)

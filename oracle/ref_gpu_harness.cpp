@@ -10,12 +10,21 @@
 // are wrong.  ref_gpu_luondevice() can hold a ballast allocation during the
 // call so that the free memory, and with it TMPMEMNUM, stays below that bound;
 // numeric.cu itself is not modified.
+//
+// LUonDevice's progress and error text goes to streams in the bad state: this
+// library links its C++ runtime statically and formatting numbers through it
+// is not possible when the library is loaded into Python.  The call is timed
+// here with CUDA events around it (the same span as its own "Total GPU time",
+// numeric.cu:431-433,621-625: allocations, copies, factorization); failure is
+// detected as the reference's Python binding does, by non-finite factor values
+// (src/glu_binding.cpp:119-127).
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <sstream>
-#include <string>
+#include <ostream>
+#include <streambuf>
 
 #include "numeric.h"
 #include "symbolic.h"
@@ -23,34 +32,61 @@
 struct RefCtx;
 extern "C" Symbolic_Matrix *ref_symbolic_matrix(RefCtx *c);
 
+namespace {
+struct NullBuf : std::streambuf {
+    int overflow(int c) override { return c; }
+};
+std::ostream &null_stream() {
+    static NullBuf buf;
+    static std::ostream os(&buf);
+    os.setstate(std::ios::badbit);
+    return os;
+}
+}  // namespace
+
 extern "C" {
 
-// Returns 0 on success, 1 when LUonDevice wrote to its error stream, 2 when the
-// ballast allocation failed.  *total_ms is LUonDevice's own "Total GPU time"
-// (it includes its allocations and copies, numeric.cu:431-433,621-625).
-int ref_gpu_luondevice(RefCtx *c, int perturb, size_t keep_free_bytes, float *total_ms,
-                       char *err_buf, int err_len) {
+// Returns 0 on success, 1 when the factors contain NaN/Inf (the reference's
+// own failure signal), 2 when the ballast allocation failed, 3 on a CUDA error
+// around the call.  *total_ms: device time of the whole LUonDevice call.
+int ref_gpu_luondevice(RefCtx *c, int perturb, size_t keep_free_bytes, float *total_ms, char *err_buf,
+                       int err_len) {
+    if (err_buf && err_len > 0) err_buf[0] = 0;
     void *ballast = nullptr;
     if (keep_free_bytes > 0) {
         size_t free_b = 0, total_b = 0;
         cudaMemGetInfo(&free_b, &total_b);
         if (free_b > keep_free_bytes) {
             if (cudaMalloc(&ballast, free_b - keep_free_bytes) != cudaSuccess) {
-                snprintf(err_buf, err_len, "ballast allocation failed");
+                if (err_buf) snprintf(err_buf, err_len, "ballast allocation failed");
                 return 2;
             }
         }
     }
-    std::ostringstream out, err;
-    LUonDevice(*ref_symbolic_matrix(c), out, err, perturb != 0);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    Symbolic_Matrix *s = ref_symbolic_matrix(c);
+    LUonDevice(*s, null_stream(), null_stream(), perturb != 0);
+    cudaEventRecord(e1, 0);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float ms = -1.0f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     if (ballast) cudaFree(ballast);
-    *total_ms = -1.0f;
-    std::string o = out.str();
-    size_t pos = o.find("Total GPU time: ");
-    if (pos != std::string::npos) *total_ms = std::stof(o.substr(pos + 16));
-    std::string e = err.str();
-    if (err_buf && err_len > 0) snprintf(err_buf, err_len, "%s", e.c_str());
-    return e.empty() ? 0 : 1;
+    *total_ms = ms;
+    if (ce != cudaSuccess) {
+        if (err_buf) snprintf(err_buf, err_len, "CUDA error: %s", cudaGetErrorString(ce));
+        return 3;
+    }
+    for (float v : s->val)
+        if (!std::isfinite(v)) {
+            if (err_buf) snprintf(err_buf, err_len, "non-finite factor values");
+            return 1;
+        }
+    return 0;
 }
 
 }  // extern "C"

@@ -171,6 +171,32 @@ void ref_solve(RefCtx *c, const float *luval, const float *rhs, float *x) {
     s->val.swap(saved);
 }
 
+// Load a Symbolic_Matrix from arrays (pattern, CSR, values, levels) without
+// running the reference's symbolic phase, e.g. to time LUonDevice on a
+// pattern whose reference fill_in would take minutes.  The arrays must be the
+// ones the reference's symbolic phase produces (the product's symbolic phase
+// produces them bit for bit).
+void ref_load_pattern(RefCtx *c, unsigned n, unsigned nnz, const unsigned *sym_c_ptr,
+                      const unsigned *sym_r_idx, const unsigned *l_col_ptr, const unsigned *csr_r_ptr,
+                      const unsigned *csr_c_idx, const unsigned *csr_diag_ptr, const float *val,
+                      int num_lev, const int *level_ptr, const int *level_idx) {
+    delete c->sym;
+    c->n = n;
+    Symbolic_Matrix *s = new Symbolic_Matrix(n, null_stream(), null_stream());
+    s->nnz = nnz;
+    s->num_lev = num_lev;
+    s->sym_c_ptr.assign(sym_c_ptr, sym_c_ptr + n + 1);
+    s->sym_r_idx.assign(sym_r_idx, sym_r_idx + nnz);
+    s->l_col_ptr.assign(l_col_ptr, l_col_ptr + n);
+    s->csr_r_ptr.assign(csr_r_ptr, csr_r_ptr + n + 1);
+    s->csr_c_idx.assign(csr_c_idx, csr_c_idx + nnz);
+    s->csr_diag_ptr.assign(csr_diag_ptr, csr_diag_ptr + n);
+    s->val.assign(val, val + nnz);
+    s->level_ptr.assign(level_ptr, level_ptr + num_lev + 1);
+    s->level_idx.assign(level_idx, level_idx + n);
+    c->sym = s;
+}
+
 // Replace the factor values held by the Symbolic_Matrix (used by the GPU
 // reference driver, which factors them in place).
 void ref_set_val(RefCtx *c, const float *val) {
