@@ -325,6 +325,13 @@ def main():
     elif dom == "k_dense_update":
         dom_bytes = float((8.0 * mp * mp + 2 * 4.0 * 64 * mp).sum()) * B
         dom_flops = float((2.0 * 64 * mp * mp).sum()) * B
+    elif dom == "k_sn_update":
+        # L21 and U12 read once, every m x nt output read and written, positions read
+        dom_bytes = float(st.sn_update_bytes) * B
+        dom_flops = float(st.sn_update_flops) * B
+    elif dom in ("k_sn_panel", "k_sn_diag"):
+        dom_bytes = float(st.sn_panel_bytes) * B
+        dom_flops = 0.0
     else:  # panel: diagonal block + L21 rows + U12 columns read and written
         dom_bytes = float((8.0 * (64 * 64 + 2 * 64 * mp)).sum()) * B
         dom_flops = float((2.0 * 64 * 64 * mp).sum()) * B
@@ -337,6 +344,7 @@ def main():
             "algorithmic_bytes": dom_bytes,
             "fp32_tflops": dom_flops / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0,
             "fp32_peak_tflops_derived": fp32_peak,
+            "fp32_frac_of_derived": (dom_flops / (dom_ms / 1e3) / 1e12) / fp32_peak if dom_ms > 0 else 0.0,
             "factor_breakdown_ms": {k: round(v[0], 4) for k, v in kt.items() if v[1]},
             "factor_fp32_tflops": flops / (factor_ms / 1e3) / 1e12}
 
@@ -344,7 +352,8 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": W["desc"], "n": n, "nnz_lu": nnz_lu, "batch": B, "nrhs": nrhs,
-                       "levels": st.num_lev, "dense_tail": st.dense_tail, "l2": "inputs larger than L2",
+                       "levels": st.num_lev, "dense_tail": st.dense_tail, "supernodes": st.supernodes,
+                       "supernode_levels": st.sn_levels, "l2": "inputs larger than L2",
                        "parallelism": f"replicas x{world}" if B == 1 else f"batch x{world}"},
             "refactor_ms": factor_ms, "solve_refined_ms": solve_ms, "residual": residual,
             "refine_iterations": iters, "refine_dtype": "f64",

@@ -76,11 +76,12 @@ static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
 // Kernel kinds of glu_factor for the optional per-kernel profile.
 enum KernelKind {
     KK_PERT = 0, KK_LEVEL, KK_CHAIN, KK_SCALE, KK_DGATHER, KK_PANEL, KK_UPDATE, KK_DSCATTER, KK_CHECK,
-    KK_SN_PANEL, KK_SN_UPDATE
+    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE
 };
 static const char *const kKindNames[GLU_KERNEL_KINDS] = {
     "k_colsum+k_pert_finish", "k_factor_level", "k_factor_chain", "k_scale_level", "k_dense_gather",
-    "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_panel", "k_sn_update"};
+    "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_diag", "k_sn_panel",
+    "k_sn_update"};
 
 // Events around every launch of one glu_factor call, when enabled.
 struct KernelProfiler {
@@ -130,7 +131,7 @@ struct KernelProfiler {
 enum StepKind { STEP_LEVEL = 0, STEP_CHAIN = 1 };
 // One level of the supernodal schedule: supernodes [i0, i1) of the level order.
 struct SnLevel {
-    uint32_t i0, i1, pblocks, ublocks, atomic;
+    uint32_t i0, i1, pblocks, ublocks, atomic, wide;  // wide: has a supernode of width >= 2
 };
 struct Step {
     int kind;
@@ -171,9 +172,8 @@ struct glu_handle_s {
     // supernodal plan of the sparse part (used when tune.sn_width != 0)
     bool use_sn = false;
     uint32_t nsn = 0;
-    DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_dscr, d_sn_scratch;
+    DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
-    uint64_t sn_scr_stride = 0;
     SnPlanDev SN{};
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
@@ -398,6 +398,7 @@ Status build_sn_plan(glu_handle_s *h) {
     h->use_sn = width > 0 && t > 0;
     h->nsn = 0;
     h->sn_levels.clear();
+    h->stats.sn_update_flops = h->stats.sn_update_bytes = h->stats.sn_panel_bytes = 0;
     if (!h->use_sn) return GLU_OK;
     auto nl = [&](uint32_t c) { return s.sym_c_ptr[c + 1] - s.l_col_ptr[c] - 1; };
     auto nu = [&](uint32_t c) { return s.csr_r_ptr[c + 1] - s.csr_diag_ptr[c] - 1; };
@@ -445,50 +446,64 @@ Status build_sn_plan(glu_handle_s *h) {
         std::vector<uint32_t> cur(lcount.begin(), lcount.end() - 1);
         for (uint32_t q = 0; q < ns; ++q) order[cur[lev[q]]++] = q;
     }
-    std::vector<uint32_t> col(ns), wid(ns), pblk(size_t(ns) + 1, 0), ublk(size_t(ns) + 1, 0), dscr(ns, 0);
-    uint64_t scr_max = 0;
-    const uint32_t PT = kSnPanelThreads, UT = 64;
+    std::vector<uint32_t> col(ns), wid(ns), pblk(size_t(ns) + 1, 0), ublk(size_t(ns) + 1, 0),
+        tgt(size_t(ns) + 1, 0);
+    std::vector<uint64_t> pos_off(size_t(ns) + 1, 0);
+    const uint32_t PT = kSnPanelThreads, UT = 64, TW = kSnPanelThreads / 32;
+    double upd_flops = 0, upd_bytes = 0, pan_bytes = 0;
     for (int32_t l = 0; l < nlev; ++l) {
-        uint64_t scr = 0;
-        uint32_t updating = 0;
+        uint32_t updating = 0, wide = 0;
         for (uint32_t i = lcount[l]; i < lcount[l + 1]; ++i) {
             const uint32_t q = order[i];
             const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
             const uint64_t m = nl(last), nt = nu(last);
             col[i] = first[q];
             wid[i] = w;
-            uint64_t pb, ub;
             const uint64_t tiles = ((m + UT - 1) / UT) * ((nt + UT - 1) / UT);
-            if (w == 1) {
-                pb = (m + PT - 1) / PT;
-                ub = tiles;
-            } else {
-                pb = 1 + (m + PT - 1) / PT + (nt + PT - 1) / PT;
-                ub = 1 + tiles;
-                dscr[i] = uint32_t(scr);
-                scr += uint64_t(w) * w;
-            }
+            const uint64_t pb = (m + PT - 1) / PT + (w >= 2 ? (nt + TW - 1) / TW : 0);
             if (tiles) ++updating;
-            if (uint64_t(pblk[i]) + pb > UINT32_MAX || uint64_t(ublk[i]) + ub > UINT32_MAX)
+            if (w >= 2) ++wide;
+            if (uint64_t(pblk[i]) + pb > UINT32_MAX || uint64_t(ublk[i]) + tiles > UINT32_MAX)
                 return set_error(GLU_ERR_UNSUPPORTED, "supernodal schedule too large");
             pblk[i + 1] = pblk[i] + uint32_t(pb);
-            ublk[i + 1] = ublk[i] + uint32_t(ub);
+            ublk[i + 1] = ublk[i] + uint32_t(tiles);
+            tgt[i + 1] = tgt[i] + uint32_t(nt);
+            pos_off[i + 1] = pos_off[i] + m * nt;
+            upd_flops += 2.0 * double(m) * w * nt;
+            upd_bytes += 4.0 * (double(m) * w + double(w) * nt) + 8.0 * double(m) * nt;
+            pan_bytes += 8.0 * (double(m) * w + double(w) * nt) + (w >= 2 ? 8.0 * w * w : 0.0);
         }
-        scr_max = std::max(scr_max, scr);
         const uint32_t i0 = lcount[l], i1 = lcount[l + 1];
-        h->sn_levels.push_back(SnLevel{i0, i1, pblk[i1] - pblk[i0], ublk[i1] - ublk[i0], updating > 1 ? 1u : 0u});
+        h->sn_levels.push_back(
+            SnLevel{i0, i1, pblk[i1] - pblk[i0], ublk[i1] - ublk[i0], updating > 1 ? 1u : 0u, wide ? 1u : 0u});
     }
     h->nsn = ns;
-    h->sn_scr_stride = std::max<uint64_t>(scr_max, 1);
     GLU_CUDA(upload(h->d_sn_col, col), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_w, wid), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pblk, pblk), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_ublk, ublk), "upload supernodes");
-    GLU_CUDA(upload(h->d_sn_dscr, dscr), "upload supernodes");
-    h->d_sn_scratch.release();
-    GLU_CUDA(h->d_sn_scratch.alloc(sizeof(float) * h->sn_scr_stride * h->batch), "allocate supernode scratch");
+    GLU_CUDA(upload(h->d_sn_pos_off, pos_off), "upload supernodes");
     h->SN = SnPlanDev{h->d_sn_col.as<uint32_t>(), h->d_sn_w.as<uint32_t>(), h->d_sn_pblk.as<uint32_t>(),
-                      h->d_sn_ublk.as<uint32_t>(), h->d_sn_dscr.as<uint32_t>()};
+                      h->d_sn_ublk.as<uint32_t>(), nullptr, h->d_sn_pos_off.as<uint64_t>()};
+    // position table of the update scatter, when it fits in a quarter of the free memory
+    h->d_sn_pos.release();
+    const uint64_t entries = pos_off[ns];
+    size_t free_b = 0, total_b = 0;
+    if (entries > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+        double(entries) * sizeof(uint32_t) <= 0.25 * double(free_b) &&
+        h->d_sn_pos.alloc(sizeof(uint32_t) * entries) == cudaSuccess) {
+        DevBuf d_tgt;
+        GLU_CUDA(upload(d_tgt, tgt), "upload supernodes");
+        GLU_CUDA(launch_sn_positions(h->P, h->SN, d_tgt.as<uint32_t>(), ns, h->d_sn_pos.as<uint32_t>(), 0),
+                 "supernode positions");
+        GLU_CUDA(cudaDeviceSynchronize(), "supernode positions");
+        h->SN.pos = h->d_sn_pos.as<uint32_t>();
+        upd_bytes += 4.0 * double(entries);
+    }
+    cudaGetLastError();
+    h->stats.sn_update_flops = upd_flops;
+    h->stats.sn_update_bytes = upd_bytes;
+    h->stats.sn_panel_bytes = pan_bytes;
     return GLU_OK;
 }
 
@@ -654,7 +669,7 @@ Status build_plan(glu_handle_s *h) {
     h->stats.sn_levels = uint32_t(h->sn_levels.size());
     uint64_t launches = 2;
     if (h->use_sn) {
-        for (const SnLevel &lv : h->sn_levels) launches += (lv.pblocks ? 1 : 0) + (lv.ublocks ? 1 : 0);
+        for (const SnLevel &lv : h->sn_levels) launches += lv.wide + (lv.pblocks ? 1 : 0) + (lv.ublocks ? 1 : 0);
     } else {
         launches += h->steps.size() + (NL ? 1 : 0);
     }
@@ -1161,17 +1176,17 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     }
     const uint32_t NL = h->use_sn ? 0u : uint32_t(h->levels_h.size());
     if (h->use_sn) {
-        float *scr = h->d_sn_scratch.as<float>() + size_t(first) * h->sn_scr_stride;
         for (const SnLevel &lv : h->sn_levels) {
+            if (lv.wide)
+                GLU_LAUNCH(KK_SN_DIAG, launch_sn_diag(h->P, h->SN, val, stride, count, pert, lv.i0, lv.i1, st),
+                           "factor (supernode diagonal blocks)");
             if (lv.pblocks)
                 GLU_LAUNCH(KK_SN_PANEL,
-                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, scr, h->sn_scr_stride, lv.i0,
-                                           lv.i1, lv.pblocks, st),
+                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, lv.i0, lv.i1, lv.pblocks, st),
                            "factor (supernode panels)");
             if (lv.ublocks)
                 GLU_LAUNCH(KK_SN_UPDATE,
-                           launch_sn_update(h->P, h->SN, val, stride, count, scr, h->sn_scr_stride, lv.i0, lv.i1,
-                                            lv.ublocks, lv.atomic, st),
+                           launch_sn_update(h->P, h->SN, val, stride, count, lv.i0, lv.i1, lv.ublocks, lv.atomic, st),
                            "factor (supernode updates)");
         }
     }

@@ -12,16 +12,16 @@
 // column the rows of the supernode present form a suffix k0..l (fill closure).
 //
 // Supernodes are leveled by the reference's column dependencies
-// (symbolic.cc:106-151) contracted to supernodes.  Per level two launches:
-//   panel:  A11 = L11 U11 (GESP pivots, numeric.cu:139-140), L21 = A21 U11^-1,
-//           U12(:, j) = L11^-1 A12(:, j) for every target j;
+// (symbolic.cc:106-151) contracted to supernodes.  Per level three launches:
+//   diag:   A11 = L11 U11 in place (GESP pivots, numeric.cu:139-140);
+//   panel:  L21 = A21 U11^-1 (a row per thread), U12(:, j) = L11^-1 A12(:, j)
+//           for every target j (a column per warp);
 //   update: A(rows of L21, j) -= L21 U12(:, j) for every target j, as 64 x 64
 //           output tiles (FP32 FMA, K = w), scattered to the CSC positions of
-//           column j found by search in its row list.
+//           column j (a position table built once per pattern, or a search in
+//           column j's row list).
 // Every entry receives the operations of the column algorithm in the same
-// column order (fused multiply-add instead of multiply and subtract).  The
-// panel blocks of a supernode each factor its diagonal block; the factored
-// block goes to scratch and the update launch stores it.
+// column order (fused multiply-add instead of multiply and subtract).
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 
@@ -62,36 +62,56 @@ __device__ __forceinline__ uint32_t seg_len(const DevPattern &P, uint32_t j, uin
     return lo;
 }
 
-// Factor the w x w diagonal block into sF (column-major, leading dimension
-// kLD): unit L11 strictly below, U11 on and above the diagonal.  Pivot c is
-// perturbed (GESP) when its column has an L part: c < w-1, or m > 0.
-// 128 threads: thread = (row, half of the columns).
-__device__ __forceinline__ void sn_factor_diag(const DevPattern &P, const float *__restrict__ val, const Sn &d,
-                                               float pert, float *sF, float *lcol) {
-    const uint32_t tid = threadIdx.x;
-    const uint32_t w = d.w;
-    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
-        const uint32_t cc = e / w, i = e - cc * w;
-        sF[cc * kLD + i] = ld_cg(val + P.diag[d.s + cc] + i - cc);
-    }
-    __syncthreads();
+// Factor the w x w diagonal block in place, register resident: 128 threads,
+// thread = (row, half of the columns) holding 32 values; row c is broadcast
+// through shared memory (double buffered, one barrier per column).  Pivot c
+// is perturbed (GESP, numeric.cu:139-140) when its column has an L part:
+// c < w-1, or m > 0.  Step c: L(i,c) = A(i,c) / U(c,c), then
+// A(i,j) -= L(i,c) U(c,j) for j > c, as in the column algorithm.
+__device__ __forceinline__ void sn_diag_regs(const DevPattern &P, float *__restrict__ val, const Sn &d, float pert,
+                                             float (*urow)[kSnMaxWidth], uint32_t *sBase) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
     const uint32_t row = tid >> 1, half = tid & 1;
-    for (uint32_t c = 0; c < w; ++c) {
-        const bool has_l = (c + 1 < w) || d.m > 0;
-        const float p = sF[c * kLD + c];
-        const float de = (has_l && pert > 0.0f && fabsf(p) < pert) ? pert : p;
-        if (half == 0 && row > c && row < w) {
-            const float l = sF[c * kLD + row] / de;
-            sF[c * kLD + row] = l;
-            lcol[row] = l;
+    const uint32_t w = d.w;
+    const bool rv = row < w;
+    if (tid < w) sBase[tid] = P.diag[d.s + tid] - tid;  // position of row s in column s + tid
+    __syncthreads();
+    float a[32];
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) {
+        const uint32_t cc = half * 32 + jj;
+        a[jj] = (rv && cc < w) ? ld_cg(val + sBase[cc] + row) : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < int(kSnMaxWidth); ++c) {
+        if (uint32_t(c) >= w) break;
+        const int hc = c >> 5, jc = c & 31;
+        float *u = urow[c & 1];
+        if (row == uint32_t(c)) {
+            if (half == uint32_t(hc)) {
+                const bool has_l = (uint32_t(c) + 1 < w) || d.m > 0;
+                float p = a[jc];
+                if (has_l && pert > 0.0f && fabsf(p) < pert) p = pert;
+                a[jc] = p;
+            }
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj)
+                if (int(half) * 32 + jj >= c) u[half * 32 + jj] = a[jj];
         }
-        if (tid == 0 && de != p) sF[c * kLD + c] = de;
         __syncthreads();
-        if (row > c && row < w) {
-            const float l = lcol[row];
-            for (uint32_t j = c + 1 + half; j < w; j += 2) sF[j * kLD + row] = fmaf(-l, sF[j * kLD + c], sF[j * kLD + row]);
+        const float lsrc = __shfl_sync(0xffffffffu, a[jc], (lane & ~1u) | uint32_t(hc));
+        if (rv && row > uint32_t(c)) {
+            const float l = lsrc / u[c];
+            if (half == uint32_t(hc)) a[jc] = l;
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj)
+                if (int(half) * 32 + jj > c) a[jj] = fmaf(-l, u[half * 32 + jj], a[jj]);
         }
-        __syncthreads();
+    }
+#pragma unroll
+    for (int jj = 0; jj < 32; ++jj) {
+        const uint32_t cc = half * 32 + jj;
+        if (rv && cc < w) st_cg(val + sBase[cc] + row, a[jj]);
     }
 }
 
@@ -116,59 +136,52 @@ __device__ __forceinline__ void sn_l21_row(float *__restrict__ val, const uint32
         if (uint32_t(c) < w) st_cg(val + sOff[c] + r, a[c]);
 }
 
-// Target column j of U12: L11 x = a over the supernode's rows present in
-// column j (a suffix of length len; the rows above it are structural zeros).
-template <int W>
-__device__ __forceinline__ void sn_u12_col(float *__restrict__ val, uint32_t pl, uint32_t len, uint32_t w,
-                                           const float *sF) {
-    float a[W];
-    const uint32_t z = w - len;  // first row present
-#pragma unroll
-    for (int k = 0; k < W; ++k) a[k] = (uint32_t(k) < w && uint32_t(k) >= z) ? ld_cg(val + pl - (w - 1 - k)) : 0.0f;
-#pragma unroll
-    for (int r = 0; r < W; ++r) {
-        if (uint32_t(r) < w && uint32_t(r) >= z) {
-            const float u = a[r];
-#pragma unroll
-            for (int i = r + 1; i < W; ++i) a[i] = fmaf(-sF[r * kLD + i], u, a[i]);  // a[i >= w] unused
-        }
+// Target column j of U12 by one warp: L11 x = a over the supernode's rows
+// present in column j (a suffix from row z; the rows above it are structural
+// zeros and stay untouched).  Lane k holds rows k and k + 32.
+__device__ __forceinline__ void sn_u12_warp(const DevPattern &P, float *__restrict__ val, const Sn &d, uint32_t jt,
+                                            const float *sF, uint32_t lane) {
+    const uint32_t e = P.rdiag[d.l] + 1 + jt;
+    const uint32_t pl = P.cpos[e];
+    const uint32_t w = d.w;
+    const uint32_t z = w - seg_len(P, P.cidx[e], pl, d.l, w);
+    const uint32_t k0 = lane, k1 = lane + 32;
+    const bool p0 = k0 < w && k0 >= z, p1 = k1 < w && k1 >= z;
+    float a0 = p0 ? ld_cg(val + pl - (w - 1 - k0)) : 0.0f;
+    float a1 = p1 ? ld_cg(val + pl - (w - 1 - k1)) : 0.0f;
+    for (uint32_t r = z; r < w; ++r) {
+        const float u = __shfl_sync(0xffffffffu, r < 32 ? a0 : a1, r & 31);
+        if (k0 > r && k0 < w) a0 = fmaf(-sF[r * kLD + k0], u, a0);
+        if (k1 > r && k1 < w) a1 = fmaf(-sF[r * kLD + k1], u, a1);
     }
-#pragma unroll
-    for (int k = 0; k < W; ++k)
-        if (uint32_t(k) < w && uint32_t(k) >= z) st_cg(val + pl - (w - 1 - k), a[k]);
-}
-
-template <int W>
-__device__ __forceinline__ void sn_panel_rows(const DevPattern &P, float *__restrict__ val, const Sn &d,
-                                              uint32_t role, uint32_t q, const uint32_t *sOff, const float *sF) {
-    const uint32_t tid = threadIdx.x;
-    if (role == 1) {
-        const uint32_t r = q * kSnPanelThreads + tid;
-        if (r < d.m) sn_l21_row<W>(val, sOff, d.w, r, sF);
-    } else {
-        const uint32_t jt = q * kSnPanelThreads + tid;
-        if (jt < d.nt) {
-            const uint32_t e = P.rdiag[d.l] + 1 + jt;
-            const uint32_t pl = P.cpos[e];
-            const uint32_t len = seg_len(P, P.cidx[e], pl, d.l, d.w);
-            sn_u12_col<W>(val, pl, len, d.w, sF);
-        }
-    }
+    if (p0) st_cg(val + pl - (w - 1 - k0), a0);
+    if (p1) st_cg(val + pl - (w - 1 - k1), a1);
 }
 
 }  // namespace
 
-// Panel launch of one level: supernodes [i0, i1) of the level order, blocks
-// S.pblk[i0] .. S.pblk[i1).  Per supernode of width w >= 2: block 0 stores the
-// factored diagonal block to scratch, then ceil(m / T) blocks of L21 rows and
-// ceil(nt / T) blocks of U12 columns (T = kSnPanelThreads).  Width 1: ceil(m / T)
-// blocks scale the column.  blockIdx.z selects the value set.
-__global__ void __launch_bounds__(kSnPanelThreads, 2) k_sn_panel(DevPattern P, SnPlanDev S, float *val_base,
-                                                                 uint64_t stride, const float *pert_z,
-                                                                 float *scr_base, uint64_t scr_stride,
-                                                                 uint32_t i0, uint32_t i1) {
+// Diagonal blocks of one level's supernodes [i0, i0 + gridDim.x), factored in
+// place (width-1 supernodes have none).  blockIdx.z selects the value set.
+__global__ void __launch_bounds__(128) k_sn_diag(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
+                                                 const float *pert_z, uint32_t i0) {
+    __shared__ float urow[2][kSnMaxWidth];
+    __shared__ uint32_t sBase[kSnMaxWidth];
+    const Sn d = sn_load(P, S, i0 + blockIdx.x);
+    if (d.w < 2) return;
+    float *val = val_base + blockIdx.z * stride;
+    const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
+    sn_diag_regs(P, val, d, pert, urow, sBase);
+}
+
+// Panel launch of one level (after its diagonal blocks): blocks S.pblk[i0] ..
+// S.pblk[i1).  Per supernode: ceil(m / 128) blocks of L21 rows (one row per
+// thread), then, for width >= 2, ceil(nt / 4) blocks of U12 target columns
+// (one column per warp).  Width 1: the blocks scale the column by its pivot
+// (numeric.cu:133-143).  blockIdx.z selects the value set.
+__global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPlanDev S, float *val_base,
+                                                              uint64_t stride, const float *pert_z, uint32_t i0,
+                                                              uint32_t i1) {
     __shared__ float sF[kSnMaxWidth * kLD];
-    __shared__ float lcol[kSnMaxWidth];
     __shared__ uint32_t sOff[kSnMaxWidth];
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
@@ -176,9 +189,8 @@ __global__ void __launch_bounds__(kSnPanelThreads, 2) k_sn_panel(DevPattern P, S
     const uint32_t i = upper_slot(S.pblk, i0, i1, b);
     const Sn d = sn_load(P, S, i);
     const uint32_t tid = threadIdx.x;
-    uint32_t t = b - S.pblk[i];
+    const uint32_t t = b - S.pblk[i];
     if (d.w == 1) {
-        // numeric.cu:133-143: pivot (perturbed when the column has an L part), L /= pivot
         const uint32_t dk = P.diag[d.s];
         const uint32_t r = t * kSnPanelThreads + tid;
         const float p = ld_cg(val + dk);
@@ -188,43 +200,43 @@ __global__ void __launch_bounds__(kSnPanelThreads, 2) k_sn_panel(DevPattern P, S
         if (t == 0 && tid == 0 && de != p) st_cg(val + dk, de);
         return;
     }
-    if (tid < d.w) sOff[tid] = P.diag[d.s + tid] + (d.l + 1 - (d.s + tid));
-    sn_factor_diag(P, val, d, pert, sF, lcol);
-    if (t == 0) {
-        float *scr = scr_base + blockIdx.z * scr_stride + S.dscr[i];
-        for (uint32_t e = tid; e < d.w * d.w; e += blockDim.x) {
-            const uint32_t cc = e / d.w, r = e - cc * d.w;
-            scr[e] = sF[cc * kLD + r];
-        }
-        return;
+    const uint32_t w = d.w;
+    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
+        const uint32_t cc = e / w, r = e - cc * w;
+        sF[cc * kLD + r] = ld_cg(val + P.diag[d.s + cc] + r - cc);
     }
-    t -= 1;
+    if (tid < w) sOff[tid] = P.diag[d.s + tid] + (d.l + 1 - (d.s + tid));
+    __syncthreads();
     const uint32_t nLb = (d.m + kSnPanelThreads - 1) / kSnPanelThreads;
-    const uint32_t role = t < nLb ? 1u : 2u;
-    const uint32_t q = role == 1 ? t : t - nLb;
-    if (d.w <= 2)
-        sn_panel_rows<2>(P, val, d, role, q, sOff, sF);
-    else if (d.w <= 4)
-        sn_panel_rows<4>(P, val, d, role, q, sOff, sF);
-    else if (d.w <= 8)
-        sn_panel_rows<8>(P, val, d, role, q, sOff, sF);
-    else if (d.w <= 16)
-        sn_panel_rows<16>(P, val, d, role, q, sOff, sF);
-    else if (d.w <= 32)
-        sn_panel_rows<32>(P, val, d, role, q, sOff, sF);
-    else
-        sn_panel_rows<64>(P, val, d, role, q, sOff, sF);
+    if (t < nLb) {
+        const uint32_t r = t * kSnPanelThreads + tid;
+        if (r >= d.m) return;
+        if (w <= 2)
+            sn_l21_row<2>(val, sOff, w, r, sF);
+        else if (w <= 4)
+            sn_l21_row<4>(val, sOff, w, r, sF);
+        else if (w <= 8)
+            sn_l21_row<8>(val, sOff, w, r, sF);
+        else if (w <= 16)
+            sn_l21_row<16>(val, sOff, w, r, sF);
+        else if (w <= 32)
+            sn_l21_row<32>(val, sOff, w, r, sF);
+        else
+            sn_l21_row<64>(val, sOff, w, r, sF);
+    } else {
+        const uint32_t jt = (t - nLb) * (kSnPanelThreads / 32) + tid / 32;
+        if (jt < d.nt) sn_u12_warp(P, val, d, jt, sF, tid & 31);
+    }
 }
 
-// Update launch of one level: blocks S.ublk[i0] .. S.ublk[i1).  Per supernode
-// of width >= 2, block 0 stores the factored diagonal block from scratch; the
-// others are the 64 x 64 tiles of the update (row tiles fastest).  Levels with
-// several supernodes accumulate with atomics (numeric.cu:82); a single
-// supernode updates each entry from one thread: C is loaded, the K products
-// are applied in column order, C is stored.
-__global__ void __launch_bounds__(256) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
-                                                   const float *scr_base, uint64_t scr_stride, uint32_t i0,
-                                                   uint32_t i1, uint32_t atomic) {
+// Update launch of one level: blocks S.ublk[i0] .. S.ublk[i1), the 64 x 64
+// tiles of every supernode's update (row tiles fastest).  Levels with several
+// supernodes accumulate with atomics (numeric.cu:82); a single supernode
+// updates each entry from one thread: C is loaded, the K products are applied
+// in column order, C is stored.  Target positions come from the precomputed
+// table S.pos when present, else from a search in column j's rows.
+__global__ void __launch_bounds__(256, 3) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
+                                                   uint32_t i0, uint32_t i1, uint32_t atomic) {
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
     __shared__ __align__(16) float sU[kSnMaxWidth][kTLd];
     __shared__ uint32_t sOff[kSnMaxWidth];
@@ -234,18 +246,7 @@ __global__ void __launch_bounds__(256) k_sn_update(DevPattern P, SnPlanDev S, fl
     const uint32_t i = upper_slot(S.ublk, i0, i1, b);
     const Sn d = sn_load(P, S, i);
     const uint32_t tid = threadIdx.x;
-    uint32_t t = b - S.ublk[i];
-    if (d.w >= 2) {
-        if (t == 0) {
-            const float *scr = scr_base + blockIdx.z * scr_stride + S.dscr[i];
-            for (uint32_t e = tid; e < d.w * d.w; e += blockDim.x) {
-                const uint32_t cc = e / d.w, r = e - cc * d.w;
-                st_cg(val + P.diag[d.s + cc] + r - cc, scr[e]);
-            }
-            return;
-        }
-        t -= 1;
-    }
+    const uint32_t t = b - S.ublk[i];
     const uint32_t w = d.w;
     const uint32_t nrt = (d.m + kTile - 1) / kTile;
     const uint32_t r0 = (t % nrt) * kTile, c0 = (t / nrt) * kTile;
@@ -277,35 +278,50 @@ __global__ void __launch_bounds__(256) k_sn_update(DevPattern P, SnPlanDev S, fl
         sU[k][jt] = (k + sLen[jt] >= w) ? ld_cg(val + sPl[jt] - (w - 1 - k)) : 0.0f;
     }
     const uint32_t tr = tid & 15, tc = tid >> 4;
-    uint32_t rowid[4];
-    const uint32_t lbase = P.diag[d.l] + 1;
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        const uint32_t r = r0 + tr * 4 + a;
-        rowid[a] = r < d.m ? __ldg(P.ridx + lbase + r) : 0u;
-    }
-    __syncthreads();
     uint32_t pos[4][4];
     float acc[4][4];
+    if (S.pos) {
+        const uint32_t *tab = S.pos + S.pos_off[i] + r0 + tr * 4;
 #pragma unroll
-    for (int bb = 0; bb < 4; ++bb) {
-        const uint32_t jt = tc * 4 + bb;
-        const bool tv = sLen[jt] != 0;
-        const uint32_t pl = sPl[jt], ex = sEx[jt];
+        for (int bb = 0; bb < 4; ++bb) {
+            const uint32_t jt = tc * 4 + bb;
+            const bool tv = sLen[jt] != 0;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const uint32_t r = r0 + tr * 4 + a;
+                pos[a][bb] = (tv && r < d.m) ? __ldg(tab + uint64_t(c0 + jt) * d.m + a) : 0xffffffffu;
+            }
+        }
+    } else {
+        uint32_t rowid[4];
+        const uint32_t lbase = P.diag[d.l] + 1;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const uint32_t r = r0 + tr * 4 + a;
-            uint32_t q = 0xffffffffu;
-            float c = 0.0f;
-            if (tv && r < d.m) {
-                q = pl + 1 + r;
-                if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, rowid[a]);
-                if (!atomic) c = ld_cg(val + q);
+            rowid[a] = r < d.m ? __ldg(P.ridx + lbase + r) : 0u;
+        }
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            const uint32_t jt = tc * 4 + bb;
+            const bool tv = sLen[jt] != 0;
+            const uint32_t pl = sPl[jt], ex = sEx[jt];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const uint32_t r = r0 + tr * 4 + a;
+                uint32_t q = 0xffffffffu;
+                if (tv && r < d.m) {
+                    q = pl + 1 + r;
+                    if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, rowid[a]);
+                }
+                pos[a][bb] = q;
             }
-            pos[a][bb] = q;
-            acc[a][bb] = c;
         }
     }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) acc[a][bb] = (!atomic && pos[a][bb] != 0xffffffffu) ? ld_cg(val + pos[a][bb]) : 0.0f;
+    __syncthreads();
     if (atomic) {
         for (uint32_t k = 0; k < w; ++k) {
             const float4 av = *reinterpret_cast<const float4 *>(&sL[k][tr * 4]);
@@ -339,20 +355,62 @@ __global__ void __launch_bounds__(256) k_sn_update(DevPattern P, SnPlanDev S, fl
     }
 }
 
+// Position table of the update scatter: for supernode i (level order) and its
+// target jt, entry pos_off[i] + jt * m + r is the CSC position of L21 row r in
+// column j (0xffffffff for a target that cannot hold the rows).  One warp per
+// (supernode, target) pair; tgt_off is the prefix of the targets.
+__global__ void __launch_bounds__(256) k_sn_positions(DevPattern P, SnPlanDev S, const uint32_t *tgt_off,
+                                                      uint32_t nsn, uint32_t *pos) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = uint64_t(gridDim.x) * (blockDim.x / 32);
+    const uint32_t total = tgt_off[nsn];
+    for (uint64_t g = uint64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32; g < total; g += nwarps) {
+        const uint32_t i = upper_slot(tgt_off, 0, nsn, uint32_t(g));
+        const uint32_t jt = uint32_t(g) - tgt_off[i];
+        const Sn d = sn_load(P, S, i);
+        const uint32_t e = P.rdiag[d.l] + 1 + jt;
+        const uint32_t j = P.cidx[e];
+        const uint32_t pl = P.cpos[e];
+        const uint32_t below = P.cptr[j + 1] - pl - 1;
+        uint32_t *out = pos + S.pos_off[i] + uint64_t(jt) * d.m;
+        const uint32_t lbase = P.diag[d.l] + 1;
+        for (uint32_t r = lane; r < d.m; r += 32) {
+            uint32_t q = 0xffffffffu;
+            if (below >= d.m) {
+                q = pl + 1 + r;
+                const uint32_t ex = below - d.m;
+                if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, __ldg(P.ridx + lbase + r));
+            }
+            out[r] = q;
+        }
+    }
+}
+
+cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
+                           const float *pert_z, uint32_t i0, uint32_t i1, cudaStream_t st) {
+    if (i1 <= i0) return cudaSuccess;
+    k_sn_diag<<<dim3(i1 - i0, 1, count), 128, 0, st>>>(P, S, val, stride, pert_z, i0);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                            const float *pert_z, float *scratch, uint64_t scr_stride, uint32_t i0, uint32_t i1,
-                            uint32_t blocks, cudaStream_t st) {
+                            const float *pert_z, uint32_t i0, uint32_t i1, uint32_t blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, 0, st>>>(P, S, val, stride, pert_z, scratch, scr_stride,
-                                                                   i0, i1);
+    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, 0, st>>>(P, S, val, stride, pert_z, i0, i1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                             const float *scratch, uint64_t scr_stride, uint32_t i0, uint32_t i1, uint32_t blocks,
-                             uint32_t atomic, cudaStream_t st) {
+                             uint32_t i0, uint32_t i1, uint32_t blocks, uint32_t atomic, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_update<<<dim3(blocks, 1, count), 256, 0, st>>>(P, S, val, stride, scratch, scr_stride, i0, i1, atomic);
+    k_sn_update<<<dim3(blocks, 1, count), 256, 0, st>>>(P, S, val, stride, i0, i1, atomic);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sn_positions(const DevPattern &P, const SnPlanDev &S, const uint32_t *tgt_off, uint32_t nsn,
+                                uint32_t *pos, cudaStream_t st) {
+    if (nsn == 0) return cudaSuccess;
+    k_sn_positions<<<148 * 16, 256, 0, st>>>(P, S, tgt_off, nsn, pos);
     return cudaGetLastError();
 }
 

@@ -197,6 +197,10 @@ typedef struct {
     float pert;                /* perturbation of the last GESP factorization     */
     uint32_t supernodes;       /* supernodes of the sparse part (0: column path)   */
     uint32_t sn_levels;        /* levels of the supernodal schedule               */
+    double sn_update_flops;    /* supernode updates: sum 2 m w nt                  */
+    double sn_update_bytes;    /* their algorithmic bytes: L21, U12 read once, the
+                                  m x nt outputs read and written (+ positions)   */
+    double sn_panel_bytes;     /* supernode panels: L21, U12 read and written      */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
 
@@ -206,7 +210,7 @@ glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
  * summed milliseconds and launch counts of the last glu_factor call (arrays
  * of GLU_KERNEL_KINDS entries; see glu_kernel_kind_name).  Off by default:
  * the events add a little time between launches. */
-#define GLU_KERNEL_KINDS 11
+#define GLU_KERNEL_KINDS 12
 glu_status glu_profile_enable(glu_handle_t h, int on);
 glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
 const char *glu_kernel_kind_name(int kind);
