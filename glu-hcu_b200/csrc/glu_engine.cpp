@@ -175,6 +175,8 @@ struct glu_handle_s {
     DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
+    DevBuf d_ss_col[2], d_ss_w[2], d_ss_blk[2];  // supernodal L and U sweeps
+    std::vector<SnSweepLevel> ss_levels[2];
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
     std::vector<SweepStep> sw_steps[4];
@@ -399,6 +401,8 @@ Status build_sn_plan(glu_handle_s *h) {
     h->nsn = 0;
     h->sn_levels.clear();
     h->stats.sn_update_flops = h->stats.sn_update_bytes = h->stats.sn_panel_bytes = 0;
+    h->S.sn[0] = SnSweepPlan{};
+    h->S.sn[1] = SnSweepPlan{};
     if (!h->use_sn) return GLU_OK;
     auto nl = [&](uint32_t c) { return s.sym_c_ptr[c + 1] - s.l_col_ptr[c] - 1; };
     auto nu = [&](uint32_t c) { return s.csr_r_ptr[c + 1] - s.csr_diag_ptr[c] - 1; };
@@ -501,6 +505,68 @@ Status build_sn_plan(glu_handle_s *h) {
         upd_bytes += 4.0 * double(entries);
     }
     cudaGetLastError();
+    // supernodal solve sweeps: L forward (waits for the supernodes whose L21
+    // rows fall in it), U backward (waits for the supernodes holding its targets)
+    for (int u = 0; u < 2; ++u) {
+        std::vector<int32_t> sl(ns, 0);
+        int32_t snl = 0;
+        for (uint32_t qq = 0; qq < ns; ++qq) {
+            const uint32_t q = u ? ns - 1 - qq : qq;
+            const uint32_t s0 = first[q], last = first[q + 1] - 1;
+            int32_t mx = -1;
+            if (!u) {
+                for (uint32_t c = s0; c <= last; ++c)
+                    for (uint32_t e = s.csr_r_ptr[c]; e < s.csr_diag_ptr[c]; ++e) {
+                        const uint32_t c2 = s.csr_c_idx[e];
+                        if (c2 < s0) mx = std::max(mx, sl[sn_of[c2]]);
+                    }
+            } else {
+                for (uint32_t e = s.csr_diag_ptr[last] + 1; e < s.csr_r_ptr[last + 1]; ++e) {
+                    const uint32_t j = s.csr_c_idx[e];
+                    if (j < t) mx = std::max(mx, sl[sn_of[j]]);
+                }
+            }
+            sl[q] = mx + 1;
+            snl = std::max(snl, mx + 2);
+        }
+        std::vector<uint32_t> lc(size_t(snl) + 1, 0);
+        for (uint32_t q = 0; q < ns; ++q) lc[sl[q] + 1]++;
+        for (int32_t l = 0; l < snl; ++l) lc[l + 1] += lc[l];
+        std::vector<uint32_t> ord(ns);
+        {
+            std::vector<uint32_t> cur(lc.begin(), lc.end() - 1);
+            for (uint32_t q = 0; q < ns; ++q) ord[cur[sl[q]]++] = q;
+        }
+        std::vector<uint32_t> scol(ns), sw(ns), sblk(size_t(ns) + 1, 0);
+        h->ss_levels[u].clear();
+        for (int32_t l = 0; l < snl; ++l) {
+            for (uint32_t i = lc[l]; i < lc[l + 1]; ++i) {
+                const uint32_t q = ord[i];
+                const uint32_t s0 = first[q], w = first[q + 1] - s0, last = first[q + 1] - 1;
+                uint64_t work;
+                if (!u) {
+                    work = (nl(last) + kSnSweepRows - 1) / kSnSweepRows;
+                } else {
+                    uint64_t above = 0;
+                    for (uint32_t c = s0; c <= last; ++c) above += (s.l_col_ptr[c] - (c - s0)) - s.sym_c_ptr[c];
+                    work = (above + kSnSweepAbove - 1) / kSnSweepAbove;
+                }
+                scol[i] = s0;
+                sw[i] = w;
+                sblk[i + 1] = sblk[i] + uint32_t(std::max<uint64_t>(work, 1));
+            }
+            h->ss_levels[u].push_back(SnSweepLevel{lc[l], lc[l + 1], sblk[lc[l + 1]] - sblk[lc[l]]});
+        }
+        GLU_CUDA(upload(h->d_ss_col[u], scol), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_w[u], sw), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_blk[u], sblk), "upload solve plan");
+        SnSweepPlan &pl = h->S.sn[u];
+        pl.col = h->d_ss_col[u].as<uint32_t>();
+        pl.w = h->d_ss_w[u].as<uint32_t>();
+        pl.blk = h->d_ss_blk[u].as<uint32_t>();
+        pl.levels = h->ss_levels[u].data();
+        pl.nlev = uint32_t(h->ss_levels[u].size());
+    }
     h->stats.sn_update_flops = upd_flops;
     h->stats.sn_update_bytes = upd_bytes;
     h->stats.sn_panel_bytes = pan_bytes;

@@ -135,6 +135,22 @@ struct SweepPlan {
 enum SweepMode : int { SWEEP_L = 0, SWEEP_U = 1, SWEEP_UT = 2, SWEEP_LT = 3 };
 constexpr uint32_t kSweepChunk = 128;
 
+// Supernodal L or U sweep (used when the factor is supernodal): supernodes
+// level by level in sweep order (first column, width, block prefix on the
+// device) and the host-side levels.
+struct SnSweepLevel {
+    uint32_t i0, i1, blocks;
+};
+struct SnSweepPlan {
+    const uint32_t *col = nullptr;
+    const uint32_t *w = nullptr;
+    const uint32_t *blk = nullptr;        // [count + 1]
+    const SnSweepLevel *levels = nullptr; // host array
+    uint32_t nlev = 0;
+};
+constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep
+constexpr uint32_t kSnSweepAbove = 1024;  // U entries per block of the U sweep
+
 struct SolvePlanDev {
     uint32_t t;                     // first column of the dense tail (n if none)
     uint32_t m;                     // order of the dense tail
@@ -142,8 +158,14 @@ struct SolvePlanDev {
     const uint32_t *tail_start;     // CSC position of the first row >= t of each tail column
     const uint32_t *tail_row_start; // CSR position of the first column >= t of each tail row
     SweepPlan sweep[4];             // L, U, U^T, L^T
+    SnSweepPlan sn[2];              // supernodal L and U sweeps (nlev == 0: column sweeps)
     uint32_t cluster;               // CTAs of the thin-level cluster kernel
 };
+
+// Supernodal sweep over the columns [0, t) (forward L, or backward U), then
+// y[0, t) = xo[0, t).
+cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
+                         float *y, float *xo, uint32_t nrhs, cudaStream_t st);
 
 // Transform in: y[j] = rhs[col_perm[piv[j]]] * (mc64 ? col_scale_perm[piv[j]] : 1)
 // (symbolic.cc:215-223); out: x[j] = y[row_perm_inv[j]] * (mc64 ? row_scale[j] : 1)

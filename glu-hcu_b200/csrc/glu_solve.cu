@@ -354,7 +354,8 @@ static cudaError_t tail_coupling(const DevPattern &P, const SolvePlanDev &S, con
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
                              uint32_t *ticket, uint32_t *status, cudaStream_t st) {
-    cudaError_t e = run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, st);
+    cudaError_t e = S.sn[0].nlev ? run_sn_sweep(P, S.sn[0], false, S.t, val, y, xo, nrhs, st)
+                                 : run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, st);
     if (e != cudaSuccess) return e;
     return dense_sweep<0>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
 }
@@ -364,7 +365,9 @@ cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float 
                         uint32_t *ticket, uint32_t *status, cudaStream_t st) {
     cudaError_t e = dense_sweep<1>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
     if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, false, st);
-    if (e == cudaSuccess) e = run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, st);
+    if (e == cudaSuccess)
+        e = S.sn[1].nlev ? run_sn_sweep(P, S.sn[1], true, S.t, val, y, xo, nrhs, st)
+                         : run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, st);
     return e;
 }
 

@@ -1,0 +1,160 @@
+// Supernodal form of the sparse L and U sweeps of the triangular solves.
+//
+// The reference sweeps column by column (Symbolic_Matrix::solve,
+// src/symbolic.cc:226-239).  With the factor's supernodes (runs of columns
+// [s, s+w) with a dense diagonal block and a common lower pattern) a sweep
+// step is a whole supernode: its w unknowns are solved against the dense
+// diagonal block (one warp, the block staged in shared memory) and their
+// off-diagonal entries are then scattered into the unknowns they feed:
+//   L (forward, unit):  x_S = L11^-1 y_S;  y_r -= L21(r,:) x_S for the m rows
+//                       below the block (one thread per row, dot over w);
+//   U (backward):       x_S = U11^-1 y_S;  y_i -= U(i,c) x_c for the entries
+//                       of the supernode's columns above the block.
+// Supernodes are leveled by the sweep's dependencies: L — a supernode waits
+// for the supernodes whose L21 rows fall in it; U — for the supernodes that
+// hold its update targets.  Finished unknowns go to xo (another block of the
+// same supernode may still read y_S) and are copied back after the sweep.
+#include "glu_common.cuh"
+#include "glu_kernels.h"
+
+namespace glu {
+
+namespace {
+constexpr int kLD = kSnMaxWidth + 1;
+}
+
+__global__ void __launch_bounds__(256) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t i0, uint32_t i1) {
+    __shared__ float sT[kSnMaxWidth * kLD];
+    __shared__ float xs[kSnMaxWidth];
+    const uint32_t b = W.blk[i0] + blockIdx.x;
+    const uint32_t i = upper_slot(W.blk, i0, i1, b);
+    const uint32_t s = W.col[i], w = W.w[i], l = s + w - 1;
+    const uint32_t lbase = P.diag[l] + 1;
+    const uint32_t m = P.cptr[l + 1] - lbase;
+    const uint32_t t = b - W.blk[i];
+    const uint32_t tid = threadIdx.x, n = P.n;
+    // L11, strictly lower: L(s+k, s+c) at diag[s+c] + (k - c)
+    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
+        const uint32_t c = e / w, k = e - c * w;
+        if (k > c) sT[c * kLD + k] = __ldg(val + P.diag[s + c] + (k - c));
+    }
+    __syncthreads();
+    const uint32_t r = t * blockDim.x + tid;  // L21 row of this thread
+    for (uint32_t q = 0; q < nrhs; ++q) {
+        float *yq = y + size_t(q) * n;
+        if (tid < 32) {
+            const uint32_t k0 = tid, k1 = tid + 32;
+            float v0 = k0 < w ? __ldcg(yq + s + k0) : 0.0f;
+            float v1 = k1 < w ? __ldcg(yq + s + k1) : 0.0f;
+            for (uint32_t c = 0; c + 1 < w; ++c) {
+                const float xc = __shfl_sync(0xffffffffu, c < 32 ? v0 : v1, c & 31);
+                if (k0 > c && k0 < w) v0 = __fsub_rn(v0, __fmul_rn(sT[c * kLD + k0], xc));
+                if (k1 > c && k1 < w) v1 = __fsub_rn(v1, __fmul_rn(sT[c * kLD + k1], xc));
+            }
+            if (k0 < w) xs[k0] = v0;
+            if (k1 < w) xs[k1] = v1;
+            if (t == 0) {
+                if (k0 < w) xo[size_t(q) * n + s + k0] = v0;
+                if (k1 < w) xo[size_t(q) * n + s + k1] = v1;
+            }
+        }
+        __syncthreads();
+        if (r < m) {
+            float acc = 0.0f;
+            for (uint32_t c = 0; c < w; ++c) acc = fmaf(__ldg(val + P.diag[s + c] + (l + 1 - (s + c)) + r), xs[c], acc);
+            if (acc != 0.0f) atomicAdd(yq + __ldg(P.ridx + lbase + r), -acc);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t i0, uint32_t i1) {
+    __shared__ float sT[kSnMaxWidth * kLD];
+    __shared__ float xs[kSnMaxWidth];
+    __shared__ uint32_t pre[kSnMaxWidth + 1];
+    const uint32_t b = W.blk[i0] + blockIdx.x;
+    const uint32_t i = upper_slot(W.blk, i0, i1, b);
+    const uint32_t s = W.col[i], w = W.w[i];
+    const uint32_t t = b - W.blk[i];
+    const uint32_t tid = threadIdx.x, n = P.n;
+    // U11 with its diagonal: U(s+k, s+c), k <= c, at diag[s+c] - (c - k)
+    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
+        const uint32_t c = e / w, k = e - c * w;
+        if (k <= c) sT[c * kLD + k] = __ldg(val + P.diag[s + c] - (c - k));
+    }
+    if (tid == 0) {
+        // entries of column s+c above the block: positions cptr[s+c] .. diag[s+c]-c-1
+        uint32_t acc = 0;
+        for (uint32_t c = 0; c < w; ++c) {
+            pre[c] = acc;
+            acc += (P.diag[s + c] - c) - P.cptr[s + c];
+        }
+        pre[w] = acc;
+    }
+    __syncthreads();
+    const uint32_t e0 = t * kSnSweepAbove, e1 = min(e0 + kSnSweepAbove, pre[w]);
+    for (uint32_t q = 0; q < nrhs; ++q) {
+        float *yq = y + size_t(q) * n;
+        if (tid < 32) {
+            const uint32_t k0 = tid, k1 = tid + 32;
+            float v0 = k0 < w ? __ldcg(yq + s + k0) : 0.0f;
+            float v1 = k1 < w ? __ldcg(yq + s + k1) : 0.0f;
+            for (uint32_t cc = w; cc-- > 0;) {
+                const float xc = __shfl_sync(0xffffffffu, cc < 32 ? v0 : v1, cc & 31) / sT[cc * kLD + cc];
+                if (k0 == cc) v0 = xc;
+                if (k1 == cc) v1 = xc;
+                if (k0 < cc) v0 = __fsub_rn(v0, __fmul_rn(sT[cc * kLD + k0], xc));
+                if (k1 < cc) v1 = __fsub_rn(v1, __fmul_rn(sT[cc * kLD + k1], xc));
+            }
+            if (k0 < w) xs[k0] = v0;
+            if (k1 < w) xs[k1] = v1;
+            if (t == 0) {
+                if (k0 < w) xo[size_t(q) * n + s + k0] = v0;
+                if (k1 < w) xo[size_t(q) * n + s + k1] = v1;
+            }
+        }
+        __syncthreads();
+        for (uint32_t e = e0 + tid; e < e1; e += blockDim.x) {
+            uint32_t lo = 0, hi = w;  // last c with pre[c] <= e
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (pre[mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const float xc = xs[lo];
+            if (xc == 0.0f) continue;
+            const uint32_t p = P.cptr[s + lo] + (e - pre[lo]);
+            atomicAdd(yq + __ldg(P.ridx + p), -__fmul_rn(__ldg(val + p), xc));
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_sn_copy(const float *__restrict__ xo, float *y, uint32_t t, uint32_t n) {
+    const size_t off = size_t(blockIdx.y) * n;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < t; j += gridDim.x * blockDim.x) y[off + j] = xo[off + j];
+}
+
+cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
+                         float *y, float *xo, uint32_t nrhs, cudaStream_t st) {
+    for (uint32_t l = 0; l < W.nlev; ++l) {
+        const SnSweepLevel &lv = W.levels[l];
+        if (lv.blocks == 0) continue;
+        if (upper)
+            k_sn_sweep_u<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.i0, lv.i1);
+        else
+            k_sn_sweep_l<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.i0, lv.i1);
+    }
+    if (t > 0) {
+        uint32_t bx = (t + 255) / 256;
+        if (bx > 1024) bx = 1024;
+        k_sn_copy<<<dim3(bx, nrhs, 1), 256, 0, st>>>(xo, y, t, P.n);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace glu

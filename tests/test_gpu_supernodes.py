@@ -77,6 +77,15 @@ def test_supernode_width_matches_oracle(name, width, tail):
     ref, p = _reference(lu)
     err = col_max_rel(v, ref, p["sym_c_ptr"])
     assert err <= FACTOR_TOL, (name, width, tail, err)
+    # the sweeps of this schedule (supernodal when width > 0): FP64-refined solve
+    import scipy.sparse as sp
+    from pyglu import synth
+
+    n = A[3]
+    b = synth.rhs_uniform(n, 1, seed=5)[0]
+    x = lu.solve(b, refine=True, tol=1e-12, maxiter=30)
+    M = sp.csc_matrix(A[:3], shape=(n, n))
+    assert np.linalg.norm(M @ x - b) / np.linalg.norm(b) <= 1e-10
 
 
 def test_supernodes_cut_the_level_count():
