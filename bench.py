@@ -265,8 +265,12 @@ def main():
     solve_ms = e0.elapsed_time(e1)
 
     # e2e through the public API with host buffers
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 5))
     if B == 1:
+        # one untimed pass: first-call allocations of the host-buffer path
+        lu.refactor(vals[0])
+        lu.solve(b_host[0].T if nrhs > 1 else b_host[0, 0], refine=True, tol=W["tol"])
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         e0.record(stream)
         for i in range(e2e_steps):
@@ -278,6 +282,9 @@ def main():
         h2d = vals[0].nbytes + b_host[0].nbytes
         d2h = b_host[0].nbytes
     else:
+        lu.refactor(vals[:B])
+        lu.solve(b_host, tol=W["tol"])
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         for i in range(e2e_steps):
             lu.refactor(vals[:B])

@@ -403,6 +403,7 @@ Status build_sn_plan(glu_handle_s *h) {
     h->stats.sn_update_flops = h->stats.sn_update_bytes = h->stats.sn_panel_bytes = 0;
     h->S.sn[0] = SnSweepPlan{};
     h->S.sn[1] = SnSweepPlan{};
+    h->stats.sn_sweep_levels = 0;
     if (!h->use_sn) return GLU_OK;
     auto nl = [&](uint32_t c) { return s.sym_c_ptr[c + 1] - s.l_col_ptr[c] - 1; };
     auto nu = [&](uint32_t c) { return s.csr_r_ptr[c + 1] - s.csr_diag_ptr[c] - 1; };
@@ -566,6 +567,7 @@ Status build_sn_plan(glu_handle_s *h) {
         pl.blk = h->d_ss_blk[u].as<uint32_t>();
         pl.levels = h->ss_levels[u].data();
         pl.nlev = uint32_t(h->ss_levels[u].size());
+        h->stats.sn_sweep_levels += pl.nlev;
     }
     h->stats.sn_update_flops = upd_flops;
     h->stats.sn_update_bytes = upd_bytes;

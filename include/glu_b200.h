@@ -201,6 +201,7 @@ typedef struct {
     double sn_update_bytes;    /* their algorithmic bytes: L21, U12 read once, the
                                   m x nt outputs read and written (+ positions)   */
     double sn_panel_bytes;     /* supernode panels: L21, U12 read and written      */
+    uint32_t sn_sweep_levels;  /* levels of the supernodal L and U solve sweeps    */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
 

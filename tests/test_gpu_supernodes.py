@@ -66,10 +66,10 @@ def test_supernode_width_matches_oracle(name, width, tail):
     lu = _factor(A, **tune)
     st = lu.stats
     if width:
-        assert st["supernodes"] > 0 and st["sn_levels"] > 0
+        assert st["supernodes"] > 0 and st["sn_levels"] > 0 and st["sn_sweep_levels"] > 0
         assert st["sn_levels"] <= lu.analysis.n
     else:
-        assert st["supernodes"] == 0
+        assert st["supernodes"] == 0 and st["sn_sweep_levels"] == 0
     if tail == "notail":
         assert st["dense_tail"] == 0
     v = lu.lu_values()
@@ -93,6 +93,7 @@ def test_supernodes_cut_the_level_count():
     A = _matrix("mesh90")
     lu = _factor(A, sn_width=64, dense_tail_min=NO_TAIL)
     assert lu.stats["sn_levels"] * 4 < lu.stats["num_lev"]
+    assert lu.stats["sn_sweep_levels"] * 2 < lu.stats["num_lev"]
 
 
 @pytest.mark.parametrize("width", [3, 64])
