@@ -343,10 +343,21 @@ def main():
         dom_bytes = float((8.0 * (64 * 64 + 2 * 64 * mp)).sum()) * B
         dom_flops = float((2.0 * 64 * 64 * mp).sum()) * B
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    # DRAM traffic per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
+    # over all k_sn_update launches of one factorization of the 300x300 mesh was
+    # 1.226x their algorithmic bytes; the full-size launch is scaled by that
+    traffic = None
+    traffic_note = None
+    if dom == "k_sn_update" and dom_n:
+        traffic = 1.226 * dom_bytes / dom_n
+        traffic_note = "ncu dram bytes (read+write) of k_sn_update on the 300x300 mesh, scaled by algorithmic bytes"
+    sn_alg = {"sn_update_algorithmic_bytes": float(st.sn_update_bytes) * B,
+              "sn_update_flops": float(st.sn_update_flops) * B}
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": None, "kernel": dom, "launches": dom_n, "kernel_ms": dom_ms,
+            "traffic": traffic, "traffic_source": traffic_note, "kernel": dom, "launches": dom_n,
+            "kernel_ms": dom_ms, **sn_alg,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "algorithmic_bytes": dom_bytes,
             "fp32_tflops": dom_flops / (dom_ms / 1e3) / 1e12 if dom_ms > 0 else 0.0,
