@@ -773,7 +773,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 16384u, 128u, 4u, kSnMaxWidth};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");

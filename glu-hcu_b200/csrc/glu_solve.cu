@@ -230,6 +230,15 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     auto T = [&](uint32_t i, uint32_t c) -> float {
         return kTrans ? val[doff[i] + c] : val[doff[c] + i];
     };
+    // the diagonal tile does not depend on x either: its loads are issued first
+    constexpr int kTilePer = kRB * kRB / 256;
+    float dv[kTilePer];
+#pragma unroll
+    for (int qq = 0; qq < kTilePer; ++qq) {
+        const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
+        const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+        dv[qq] = (rb0 + i < rb1 && rb0 + cc < rb1) ? T(rb0 + i, rb0 + cc) : 0.0f;
+    }
     for (uint32_t rc0 = 0; rc0 < nrhs; rc0 += kRHSChunk) {
         const uint32_t nr = min(uint32_t(kRHSChunk), nrhs - rc0);
         const uint32_t row = tid & (kRB - 1), q = tid / kRB;  // 4 quarters of 16 columns
@@ -238,23 +247,25 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
         for (uint32_t s = 0; s < tk; ++s) {
             const uint32_t c = kLower ? s : nb - 1 - s;
             const uint32_t cb0 = c * kRB, cb1 = min(cb0 + kRB, m);
+            // stage tile T(rb0.., cb0..): it does not depend on x, so it is
+            // loaded before waiting for block c, all loads of a thread in flight
+            {
+                float tv[kTilePer];
+#pragma unroll
+                for (int qq = 0; qq < kTilePer; ++qq) {
+                    const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;  // coalesced along bb
+                    const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+                    tv[qq] = (rb0 + i < rb1 && cb0 + cc < cb1) ? T(rb0 + i, cb0 + cc) : 0.0f;
+                }
+#pragma unroll
+                for (int qq = 0; qq < kTilePer; ++qq) {
+                    const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
+                    const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+                    tile[i][cc] = tv[qq];
+                }
+            }
             if (tid == 0) wait_count(flags + c, 1u, status);
             __syncthreads();
-            // stage tile T(rb0.., cb0..) and x(cb0..)
-            for (uint32_t e = tid; e < kRB * kRB; e += 256) {
-                uint32_t a = e / kRB, bb = e % kRB;  // coalesced along bb
-                uint32_t i, cc;
-                if (kTrans) {
-                    i = a;
-                    cc = bb;
-                } else {
-                    cc = a;
-                    i = bb;
-                }
-                float v = 0.0f;
-                if (rb0 + i < rb1 && cb0 + cc < cb1) v = T(rb0 + i, cb0 + cc);
-                tile[i][cc] = v;
-            }
             for (uint32_t e = tid; e < kRB * kRHSChunk; e += 256) {
                 uint32_t cc = e / kRHSChunk, r = e % kRHSChunk;
                 float v = 0.0f;
@@ -272,20 +283,12 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
         }
 #pragma unroll
         for (int r = 0; r < kRHSChunk; ++r) part[q][row][r] = acc[r];
-        // diagonal tile
-        for (uint32_t e = tid; e < kRB * kRB; e += 256) {
-            uint32_t a = e / kRB, bb = e % kRB;
-            uint32_t i, cc;
-            if (kTrans) {
-                i = a;
-                cc = bb;
-            } else {
-                cc = a;
-                i = bb;
-            }
-            float v = 0.0f;
-            if (rb0 + i < rb1 && rb0 + cc < rb1) v = T(rb0 + i, rb0 + cc);
-            tile[i][cc] = v;
+        // diagonal tile (its loads were issued at the start)
+#pragma unroll
+        for (int qq = 0; qq < kTilePer; ++qq) {
+            const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
+            const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+            tile[i][cc] = dv[qq];
         }
         __syncthreads();
         // one warp per right-hand side solves the diagonal tile
