@@ -175,7 +175,7 @@ struct glu_handle_s {
     DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
-    DevBuf d_ss_col[2], d_ss_w[2], d_ss_blk[2];  // supernodal L and U sweeps
+    DevBuf d_ss_map[2], d_ss_meta[2];  // supernodal L and U sweeps
     std::vector<SnSweepLevel> ss_levels[2];
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
@@ -538,33 +538,35 @@ Status build_sn_plan(glu_handle_s *h) {
             std::vector<uint32_t> cur(lc.begin(), lc.end() - 1);
             for (uint32_t q = 0; q < ns; ++q) ord[cur[sl[q]]++] = q;
         }
-        std::vector<uint32_t> scol(ns), sw(ns), sblk(size_t(ns) + 1, 0);
+        std::vector<uint4> smeta(ns);
+        std::vector<uint2> smap;
         h->ss_levels[u].clear();
         for (int32_t l = 0; l < snl; ++l) {
+            const uint32_t b0 = uint32_t(smap.size());
             for (uint32_t i = lc[l]; i < lc[l + 1]; ++i) {
                 const uint32_t q = ord[i];
                 const uint32_t s0 = first[q], w = first[q + 1] - s0, last = first[q + 1] - 1;
                 uint64_t work;
                 if (!u) {
+                    smeta[i] = make_uint4(s0, w, s.l_col_ptr[last] + 1, nl(last));
                     work = (nl(last) + kSnSweepRows - 1) / kSnSweepRows;
                 } else {
                     uint64_t above = 0;
                     for (uint32_t c = s0; c <= last; ++c) above += (s.l_col_ptr[c] - (c - s0)) - s.sym_c_ptr[c];
+                    smeta[i] = make_uint4(s0, w, 0u, 0u);
                     work = (above + kSnSweepAbove - 1) / kSnSweepAbove;
                 }
-                scol[i] = s0;
-                sw[i] = w;
-                sblk[i + 1] = sblk[i] + uint32_t(std::max<uint64_t>(work, 1));
+                work = std::max<uint64_t>(work, 1);
+                if (smap.size() + work > UINT32_MAX) return set_error(GLU_ERR_UNSUPPORTED, "solve schedule too large");
+                for (uint64_t bb = 0; bb < work; ++bb) smap.push_back(make_uint2(i, uint32_t(bb)));
             }
-            h->ss_levels[u].push_back(SnSweepLevel{lc[l], lc[l + 1], sblk[lc[l + 1]] - sblk[lc[l]]});
+            h->ss_levels[u].push_back(SnSweepLevel{b0, uint32_t(smap.size()) - b0});
         }
-        GLU_CUDA(upload(h->d_ss_col[u], scol), "upload solve plan");
-        GLU_CUDA(upload(h->d_ss_w[u], sw), "upload solve plan");
-        GLU_CUDA(upload(h->d_ss_blk[u], sblk), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_map[u], smap), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_meta[u], smeta), "upload solve plan");
         SnSweepPlan &pl = h->S.sn[u];
-        pl.col = h->d_ss_col[u].as<uint32_t>();
-        pl.w = h->d_ss_w[u].as<uint32_t>();
-        pl.blk = h->d_ss_blk[u].as<uint32_t>();
+        pl.map = h->d_ss_map[u].as<uint2>();
+        pl.meta = h->d_ss_meta[u].as<uint4>();
         pl.levels = h->ss_levels[u].data();
         pl.nlev = uint32_t(h->ss_levels[u].size());
         h->stats.sn_sweep_levels += pl.nlev;

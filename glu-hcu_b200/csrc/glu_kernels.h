@@ -135,17 +135,17 @@ struct SweepPlan {
 enum SweepMode : int { SWEEP_L = 0, SWEEP_U = 1, SWEEP_UT = 2, SWEEP_LT = 3 };
 constexpr uint32_t kSweepChunk = 128;
 
-// Supernodal L or U sweep (used when the factor is supernodal): supernodes
-// level by level in sweep order (first column, width, block prefix on the
-// device) and the host-side levels.
+// Supernodal L or U sweep (used when the factor is supernodal): per block of
+// the sweep (levels one after another) its supernode and part, per supernode
+// (sweep order) its record {first column, width, L: first L21 position,
+// L: L21 rows}; the host-side levels.
 struct SnSweepLevel {
-    uint32_t i0, i1, blocks;
+    uint32_t b0, blocks;  // first block, blocks
 };
 struct SnSweepPlan {
-    const uint32_t *col = nullptr;
-    const uint32_t *w = nullptr;
-    const uint32_t *blk = nullptr;        // [count + 1]
-    const SnSweepLevel *levels = nullptr; // host array
+    const uint2 *map = nullptr;
+    const uint4 *meta = nullptr;
+    const SnSweepLevel *levels = nullptr;  // host array
     uint32_t nlev = 0;
 };
 constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep

@@ -14,6 +14,7 @@
 // for the supernodes whose L21 rows fall in it; U — for the supernodes that
 // hold its update targets.  Finished unknowns go to xo (another block of the
 // same supernode may still read y_S) and are copied back after the sweep.
+// Every block finds its supernode and part through a precomputed map.
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 
@@ -24,15 +25,13 @@ constexpr int kLD = kSnMaxWidth + 1;
 }
 
 __global__ void __launch_bounds__(256) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
-                                                    float *y, float *xo, uint32_t nrhs, uint32_t i0, uint32_t i1) {
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0) {
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
-    const uint32_t b = W.blk[i0] + blockIdx.x;
-    const uint32_t i = upper_slot(W.blk, i0, i1, b);
-    const uint32_t s = W.col[i], w = W.w[i], l = s + w - 1;
-    const uint32_t lbase = P.diag[l] + 1;
-    const uint32_t m = P.cptr[l + 1] - lbase;
-    const uint32_t t = b - W.blk[i];
+    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint4 md = W.meta[bi.x];
+    const uint32_t s = md.x, w = md.y, lbase = md.z, m = md.w, t = bi.y;
+    const uint32_t l = s + w - 1;
     const uint32_t tid = threadIdx.x, n = P.n;
     // L11, strictly lower: L(s+k, s+c) at diag[s+c] + (k - c)
     for (uint32_t e = tid; e < w * w; e += blockDim.x) {
@@ -70,14 +69,12 @@ __global__ void __launch_bounds__(256) k_sn_sweep_l(DevPattern P, SnSweepPlan W,
 }
 
 __global__ void __launch_bounds__(256) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
-                                                    float *y, float *xo, uint32_t nrhs, uint32_t i0, uint32_t i1) {
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0) {
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     __shared__ uint32_t pre[kSnMaxWidth + 1];
-    const uint32_t b = W.blk[i0] + blockIdx.x;
-    const uint32_t i = upper_slot(W.blk, i0, i1, b);
-    const uint32_t s = W.col[i], w = W.w[i];
-    const uint32_t t = b - W.blk[i];
+    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint32_t s = W.meta[bi.x].x, w = W.meta[bi.x].y, t = bi.y;
     const uint32_t tid = threadIdx.x, n = P.n;
     // U11 with its diagonal: U(s+k, s+c), k <= c, at diag[s+c] - (c - k)
     for (uint32_t e = tid; e < w * w; e += blockDim.x) {
@@ -145,9 +142,9 @@ cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, 
         const SnSweepLevel &lv = W.levels[l];
         if (lv.blocks == 0) continue;
         if (upper)
-            k_sn_sweep_u<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.i0, lv.i1);
+            k_sn_sweep_u<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0);
         else
-            k_sn_sweep_l<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.i0, lv.i1);
+            k_sn_sweep_l<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0);
     }
     if (t > 0) {
         uint32_t bx = (t + 255) / 256;
