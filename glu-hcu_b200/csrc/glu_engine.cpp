@@ -131,7 +131,10 @@ struct KernelProfiler {
 enum StepKind { STEP_LEVEL = 0, STEP_CHAIN = 1 };
 // One level of the supernodal schedule: supernodes [i0, i1) of the level order.
 struct SnLevel {
-    uint32_t i0, i1, pblocks, ublocks, atomic, wide;  // wide: has a supernode of width >= 2
+    uint32_t i0, i1;        // supernodes (level order)
+    uint32_t pb0, pblocks;  // blocks in the panel map
+    uint32_t ub0, ublocks;  // tiles in the update map
+    uint32_t atomic, wide;  // wide: has a supernode of width >= 2
 };
 struct Step {
     int kind;
@@ -172,7 +175,7 @@ struct glu_handle_s {
     // supernodal plan of the sparse part (used when tune.sn_width != 0)
     bool use_sn = false;
     uint32_t nsn = 0;
-    DevBuf d_sn_col, d_sn_w, d_sn_pblk, d_sn_ublk, d_sn_pos, d_sn_pos_off;
+    DevBuf d_sn_meta, d_sn_pmap, d_sn_umap, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
     DevBuf d_ss_map[2], d_ss_meta[2];  // supernodal L and U sweeps
@@ -451,27 +454,29 @@ Status build_sn_plan(glu_handle_s *h) {
         std::vector<uint32_t> cur(lcount.begin(), lcount.end() - 1);
         for (uint32_t q = 0; q < ns; ++q) order[cur[lev[q]]++] = q;
     }
-    std::vector<uint32_t> col(ns), wid(ns), pblk(size_t(ns) + 1, 0), ublk(size_t(ns) + 1, 0),
-        tgt(size_t(ns) + 1, 0);
+    std::vector<uint4> meta(ns);
+    std::vector<uint2> pmap, umap;
+    std::vector<uint32_t> tgt(size_t(ns) + 1, 0);
     std::vector<uint64_t> pos_off(size_t(ns) + 1, 0);
     const uint32_t PT = kSnPanelThreads, UT = 64, TW = kSnPanelThreads / 32;
     double upd_flops = 0, upd_bytes = 0, pan_bytes = 0;
     for (int32_t l = 0; l < nlev; ++l) {
         uint32_t updating = 0, wide = 0;
+        const uint32_t pb0 = uint32_t(pmap.size()), ub0 = uint32_t(umap.size());
         for (uint32_t i = lcount[l]; i < lcount[l + 1]; ++i) {
             const uint32_t q = order[i];
             const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
             const uint64_t m = nl(last), nt = nu(last);
-            col[i] = first[q];
-            wid[i] = w;
+            meta[i] = make_uint4(first[q], w, uint32_t(m), uint32_t(nt));
             const uint64_t tiles = ((m + UT - 1) / UT) * ((nt + UT - 1) / UT);
             const uint64_t pb = (m + PT - 1) / PT + (w >= 2 ? (nt + TW - 1) / TW : 0);
             if (tiles) ++updating;
             if (w >= 2) ++wide;
-            if (uint64_t(pblk[i]) + pb > UINT32_MAX || uint64_t(ublk[i]) + tiles > UINT32_MAX)
+            if (pmap.size() + pb > UINT32_MAX || umap.size() + tiles > UINT32_MAX ||
+                uint64_t(tgt[i]) + nt > UINT32_MAX)
                 return set_error(GLU_ERR_UNSUPPORTED, "supernodal schedule too large");
-            pblk[i + 1] = pblk[i] + uint32_t(pb);
-            ublk[i + 1] = ublk[i] + uint32_t(tiles);
+            for (uint64_t bb = 0; bb < pb; ++bb) pmap.push_back(make_uint2(i, uint32_t(bb)));
+            for (uint64_t bb = 0; bb < tiles; ++bb) umap.push_back(make_uint2(i, uint32_t(bb)));
             tgt[i + 1] = tgt[i] + uint32_t(nt);
             pos_off[i + 1] = pos_off[i] + m * nt;
             upd_flops += 2.0 * double(m) * w * nt;
@@ -479,17 +484,21 @@ Status build_sn_plan(glu_handle_s *h) {
             pan_bytes += 8.0 * (double(m) * w + double(w) * nt) + (w >= 2 ? 8.0 * w * w : 0.0);
         }
         const uint32_t i0 = lcount[l], i1 = lcount[l + 1];
-        h->sn_levels.push_back(
-            SnLevel{i0, i1, pblk[i1] - pblk[i0], ublk[i1] - ublk[i0], updating > 1 ? 1u : 0u, wide ? 1u : 0u});
+        h->sn_levels.push_back(SnLevel{i0, i1, pb0, uint32_t(pmap.size()) - pb0, ub0, uint32_t(umap.size()) - ub0,
+                                       updating > 1 ? 1u : 0u, wide ? 1u : 0u});
     }
     h->nsn = ns;
-    GLU_CUDA(upload(h->d_sn_col, col), "upload supernodes");
-    GLU_CUDA(upload(h->d_sn_w, wid), "upload supernodes");
-    GLU_CUDA(upload(h->d_sn_pblk, pblk), "upload supernodes");
-    GLU_CUDA(upload(h->d_sn_ublk, ublk), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_meta, meta), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_pmap, pmap), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_umap, umap), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_tgt_off, tgt), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pos_off, pos_off), "upload supernodes");
-    h->SN = SnPlanDev{h->d_sn_col.as<uint32_t>(), h->d_sn_w.as<uint32_t>(), h->d_sn_pblk.as<uint32_t>(),
-                      h->d_sn_ublk.as<uint32_t>(), nullptr, h->d_sn_pos_off.as<uint64_t>()};
+    GLU_CUDA(h->d_sn_tgt.alloc(sizeof(uint4) * std::max<uint32_t>(tgt[ns], 1)), "allocate supernode targets");
+    h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),    h->d_sn_pmap.as<uint2>(), h->d_sn_umap.as<uint2>(),
+                      h->d_sn_tgt_off.as<uint32_t>(), h->d_sn_tgt.as<uint4>(), nullptr,
+                      h->d_sn_pos_off.as<uint64_t>()};
+    GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
+    GLU_CUDA(cudaDeviceSynchronize(), "supernode targets");
     // position table of the update scatter, when it fits in a quarter of the free memory
     h->d_sn_pos.release();
     const uint64_t entries = pos_off[ns];
@@ -497,10 +506,7 @@ Status build_sn_plan(glu_handle_s *h) {
     if (entries > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
         double(entries) * sizeof(uint32_t) <= 0.25 * double(free_b) &&
         h->d_sn_pos.alloc(sizeof(uint32_t) * entries) == cudaSuccess) {
-        DevBuf d_tgt;
-        GLU_CUDA(upload(d_tgt, tgt), "upload supernodes");
-        GLU_CUDA(launch_sn_positions(h->P, h->SN, d_tgt.as<uint32_t>(), ns, h->d_sn_pos.as<uint32_t>(), 0),
-                 "supernode positions");
+        GLU_CUDA(launch_sn_positions(h->P, h->SN, ns, h->d_sn_pos.as<uint32_t>(), 0), "supernode positions");
         GLU_CUDA(cudaDeviceSynchronize(), "supernode positions");
         h->SN.pos = h->d_sn_pos.as<uint32_t>();
         upd_bytes += 4.0 * double(entries);
@@ -1252,11 +1258,11 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
                            "factor (supernode diagonal blocks)");
             if (lv.pblocks)
                 GLU_LAUNCH(KK_SN_PANEL,
-                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, lv.i0, lv.i1, lv.pblocks, st),
+                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, lv.pb0, lv.pblocks, st),
                            "factor (supernode panels)");
             if (lv.ublocks)
                 GLU_LAUNCH(KK_SN_UPDATE,
-                           launch_sn_update(h->P, h->SN, val, stride, count, lv.i0, lv.i1, lv.ublocks, lv.atomic, st),
+                           launch_sn_update(h->P, h->SN, val, stride, count, lv.ub0, lv.ublocks, lv.atomic, st),
                            "factor (supernode updates)");
         }
     }

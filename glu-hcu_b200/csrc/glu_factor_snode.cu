@@ -37,13 +37,14 @@ struct Sn {
     uint32_t s, w, l, m, nt;
 };
 
-__device__ __forceinline__ Sn sn_load(const DevPattern &P, const SnPlanDev &S, uint32_t i) {
+__device__ __forceinline__ Sn sn_load(const SnPlanDev &S, uint32_t i) {
+    const uint4 r = S.meta[i];
     Sn d;
-    d.s = S.sn_col[i];
-    d.w = S.sn_w[i];
+    d.s = r.x;
+    d.w = r.y;
     d.l = d.s + d.w - 1;
-    d.m = P.cptr[d.l + 1] - P.diag[d.l] - 1;
-    d.nt = P.rptr[d.l + 1] - P.rdiag[d.l] - 1;
+    d.m = r.z;
+    d.nt = r.w;
     return d;
 }
 
@@ -139,12 +140,11 @@ __device__ __forceinline__ void sn_l21_row(float *__restrict__ val, const uint32
 // Target column j of U12 by one warp: L11 x = a over the supernode's rows
 // present in column j (a suffix from row z; the rows above it are structural
 // zeros and stay untouched).  Lane k holds rows k and k + 32.
-__device__ __forceinline__ void sn_u12_warp(const DevPattern &P, float *__restrict__ val, const Sn &d, uint32_t jt,
-                                            const float *sF, uint32_t lane) {
-    const uint32_t e = P.rdiag[d.l] + 1 + jt;
-    const uint32_t pl = P.cpos[e];
+__device__ __forceinline__ void sn_u12_warp(float *__restrict__ val, const Sn &d, uint4 g, const float *sF,
+                                            uint32_t lane) {
+    const uint32_t pl = g.x;
     const uint32_t w = d.w;
-    const uint32_t z = w - seg_len(P, P.cidx[e], pl, d.l, w);
+    const uint32_t z = w - g.y;
     const uint32_t k0 = lane, k1 = lane + 32;
     const bool p0 = k0 < w && k0 >= z, p1 = k1 < w && k1 >= z;
     float a0 = p0 ? ld_cg(val + pl - (w - 1 - k0)) : 0.0f;
@@ -166,30 +166,28 @@ __global__ void __launch_bounds__(128) k_sn_diag(DevPattern P, SnPlanDev S, floa
                                                  const float *pert_z, uint32_t i0) {
     __shared__ float urow[2][kSnMaxWidth];
     __shared__ uint32_t sBase[kSnMaxWidth];
-    const Sn d = sn_load(P, S, i0 + blockIdx.x);
+    const Sn d = sn_load(S, i0 + blockIdx.x);
     if (d.w < 2) return;
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
     sn_diag_regs(P, val, d, pert, urow, sBase);
 }
 
-// Panel launch of one level (after its diagonal blocks): blocks S.pblk[i0] ..
-// S.pblk[i1).  Per supernode: ceil(m / 128) blocks of L21 rows (one row per
+// Panel launch of one level (after its diagonal blocks): blocks [b0, b0 +
+// gridDim.x) of the panel map.  Per supernode: ceil(m / 128) blocks of L21 rows (one row per
 // thread), then, for width >= 2, ceil(nt / 4) blocks of U12 target columns
 // (one column per warp).  Width 1: the blocks scale the column by its pivot
 // (numeric.cu:133-143).  blockIdx.z selects the value set.
 __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPlanDev S, float *val_base,
-                                                              uint64_t stride, const float *pert_z, uint32_t i0,
-                                                              uint32_t i1) {
+                                                              uint64_t stride, const float *pert_z, uint32_t b0) {
     __shared__ float sF[kSnMaxWidth * kLD];
     __shared__ uint32_t sOff[kSnMaxWidth];
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
-    const uint32_t b = S.pblk[i0] + blockIdx.x;
-    const uint32_t i = upper_slot(S.pblk, i0, i1, b);
-    const Sn d = sn_load(P, S, i);
+    const uint2 bi = S.pmap[b0 + blockIdx.x];
+    const uint32_t i = bi.x, t = bi.y;
+    const Sn d = sn_load(S, i);
     const uint32_t tid = threadIdx.x;
-    const uint32_t t = b - S.pblk[i];
     if (d.w == 1) {
         const uint32_t dk = P.diag[d.s];
         const uint32_t r = t * kSnPanelThreads + tid;
@@ -201,11 +199,25 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
         return;
     }
     const uint32_t w = d.w;
-    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
-        const uint32_t cc = e / w, r = e - cc * w;
-        sF[cc * kLD + r] = ld_cg(val + P.diag[d.s + cc] + r - cc);
+    if (tid < w) sOff[tid] = P.diag[d.s + tid];
+    __syncthreads();
+    // the factored diagonal block, eight independent loads in flight per thread
+    for (uint32_t e0 = 0; e0 < kSnMaxWidth * kSnMaxWidth; e0 += 8 * kSnPanelThreads) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t e = e0 + q * kSnPanelThreads + tid, cc = e >> 6, r = e & 63;
+            v[q] = (cc < w && r < w) ? ld_cg(val + sOff[cc] + r - cc) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t e = e0 + q * kSnPanelThreads + tid, cc = e >> 6, r = e & 63;
+            if (cc < w && r < w) sF[cc * kLD + r] = v[q];
+        }
+        if (e0 + 8 * kSnPanelThreads >= w * kSnMaxWidth) break;
     }
-    if (tid < w) sOff[tid] = P.diag[d.s + tid] + (d.l + 1 - (d.s + tid));
+    __syncthreads();
+    if (tid < w) sOff[tid] += d.l + 1 - (d.s + tid);
     __syncthreads();
     const uint32_t nLb = (d.m + kSnPanelThreads - 1) / kSnPanelThreads;
     if (t < nLb) {
@@ -225,28 +237,30 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
             sn_l21_row<64>(val, sOff, w, r, sF);
     } else {
         const uint32_t jt = (t - nLb) * (kSnPanelThreads / 32) + tid / 32;
-        if (jt < d.nt) sn_u12_warp(P, val, d, jt, sF, tid & 31);
+        if (jt < d.nt) {
+            const uint4 g = S.tgt[S.tgt_off[i] + jt];
+            if (g.y != 0) sn_u12_warp(val, d, g, sF, tid & 31);
+        }
     }
 }
 
-// Update launch of one level: blocks S.ublk[i0] .. S.ublk[i1), the 64 x 64
-// tiles of every supernode's update (row tiles fastest).  Levels with several
+// Update launch of one level: blocks [b0, b0 + gridDim.x) of the update map,
+// the 64 x 64 tiles of every supernode's update (row tiles fastest).  Levels with several
 // supernodes accumulate with atomics (numeric.cu:82); a single supernode
 // updates each entry from one thread: C is loaded, the K products are applied
 // in column order, C is stored.  Target positions come from the precomputed
 // table S.pos when present, else from a search in column j's rows.
 __global__ void __launch_bounds__(256, 3) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
-                                                   uint32_t i0, uint32_t i1, uint32_t atomic) {
+                                                      uint32_t b0, uint32_t atomic) {
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
     __shared__ __align__(16) float sU[kSnMaxWidth][kTLd];
     __shared__ uint32_t sOff[kSnMaxWidth];
     __shared__ uint32_t sPl[kTile], sLen[kTile], sEx[kTile];
     float *val = val_base + blockIdx.z * stride;
-    const uint32_t b = S.ublk[i0] + blockIdx.x;
-    const uint32_t i = upper_slot(S.ublk, i0, i1, b);
-    const Sn d = sn_load(P, S, i);
+    const uint2 bi = S.umap[b0 + blockIdx.x];
+    const uint32_t i = bi.x, t = bi.y;
+    const Sn d = sn_load(S, i);
     const uint32_t tid = threadIdx.x;
-    const uint32_t t = b - S.ublk[i];
     const uint32_t w = d.w;
     const uint32_t nrt = (d.m + kTile - 1) / kTile;
     const uint32_t r0 = (t % nrt) * kTile, c0 = (t / nrt) * kTile;
@@ -255,14 +269,10 @@ __global__ void __launch_bounds__(256, 3) k_sn_update(DevPattern P, SnPlanDev S,
         const uint32_t jt = c0 + tid;
         uint32_t pl = 0, len = 0, ex = 0;
         if (jt < d.nt) {
-            const uint32_t e = P.rdiag[d.l] + 1 + jt;
-            const uint32_t j = P.cidx[e];
-            pl = P.cpos[e];
-            const uint32_t below = P.cptr[j + 1] - pl - 1;
-            if (below >= d.m) {  // always, for a pattern closed under fill
-                len = seg_len(P, j, pl, d.l, w);
-                ex = below - d.m;  // rows of column j below l that are not in L21
-            }
+            const uint4 g = S.tgt[S.tgt_off[i] + jt];
+            pl = g.x;
+            len = g.y;
+            ex = g.z;
         }
         sPl[tid] = pl;
         sLen[tid] = len;
@@ -355,31 +365,48 @@ __global__ void __launch_bounds__(256, 3) k_sn_update(DevPattern P, SnPlanDev S,
     }
 }
 
-// Position table of the update scatter: for supernode i (level order) and its
-// target jt, entry pos_off[i] + jt * m + r is the CSC position of L21 row r in
-// column j (0xffffffff for a target that cannot hold the rows).  One warp per
-// (supernode, target) pair; tgt_off is the prefix of the targets.
-__global__ void __launch_bounds__(256) k_sn_positions(DevPattern P, SnPlanDev S, const uint32_t *tgt_off,
-                                                      uint32_t nsn, uint32_t *pos) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t nwarps = uint64_t(gridDim.x) * (blockDim.x / 32);
-    const uint32_t total = tgt_off[nsn];
-    for (uint64_t g = uint64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32; g < total; g += nwarps) {
-        const uint32_t i = upper_slot(tgt_off, 0, nsn, uint32_t(g));
-        const uint32_t jt = uint32_t(g) - tgt_off[i];
-        const Sn d = sn_load(P, S, i);
-        const uint32_t e = P.rdiag[d.l] + 1 + jt;
+// Target metadata, one thread per (supernode, target) pair g (level order,
+// S.tgt_off the prefix): {CSC position pl of the supernode's last row l in
+// target column j, rows of the supernode present in column j (0: the column
+// cannot hold the L21 rows), rows of column j below l that are not L21 rows}.
+__global__ void __launch_bounds__(256) k_sn_targets(DevPattern P, SnPlanDev S, uint32_t nsn, uint4 *tgt) {
+    const uint32_t total = S.tgt_off[nsn];
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        const uint32_t i = upper_slot(S.tgt_off, 0, nsn, g);
+        const Sn d = sn_load(S, i);
+        const uint32_t e = P.rdiag[d.l] + 1 + (g - S.tgt_off[i]);
         const uint32_t j = P.cidx[e];
         const uint32_t pl = P.cpos[e];
         const uint32_t below = P.cptr[j + 1] - pl - 1;
+        uint4 o = make_uint4(pl, 0u, 0u, 0u);
+        if (below >= d.m) {  // always, for a pattern closed under fill
+            o.y = seg_len(P, j, pl, d.l, d.w);
+            o.z = below - d.m;
+        }
+        tgt[g] = o;
+    }
+}
+
+// Position table of the update scatter: for supernode i (level order) and its
+// target jt, entry pos_off[i] + jt * m + r is the CSC position of L21 row r in
+// column j (0xffffffff for a target that cannot hold the rows).  One warp per
+// (supernode, target) pair.
+__global__ void __launch_bounds__(256) k_sn_positions(DevPattern P, SnPlanDev S, uint32_t nsn, uint32_t *pos) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = uint64_t(gridDim.x) * (blockDim.x / 32);
+    const uint32_t total = S.tgt_off[nsn];
+    for (uint64_t g = uint64_t(blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32; g < total; g += nwarps) {
+        const uint32_t i = upper_slot(S.tgt_off, 0, nsn, uint32_t(g));
+        const uint32_t jt = uint32_t(g) - S.tgt_off[i];
+        const Sn d = sn_load(S, i);
+        const uint4 o = S.tgt[g];
         uint32_t *out = pos + S.pos_off[i] + uint64_t(jt) * d.m;
         const uint32_t lbase = P.diag[d.l] + 1;
         for (uint32_t r = lane; r < d.m; r += 32) {
             uint32_t q = 0xffffffffu;
-            if (below >= d.m) {
-                q = pl + 1 + r;
-                const uint32_t ex = below - d.m;
-                if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, __ldg(P.ridx + lbase + r));
+            if (o.y != 0) {
+                q = o.x + 1 + r;
+                if (o.z) q = lower_bound_u32(P.ridx, q, q + o.z + 1, __ldg(P.ridx + lbase + r));
             }
             out[r] = q;
         }
@@ -394,23 +421,29 @@ cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, 
 }
 
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                            const float *pert_z, uint32_t i0, uint32_t i1, uint32_t blocks, cudaStream_t st) {
+                            const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, 0, st>>>(P, S, val, stride, pert_z, i0, i1);
+    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, 0, st>>>(P, S, val, stride, pert_z, b0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                             uint32_t i0, uint32_t i1, uint32_t blocks, uint32_t atomic, cudaStream_t st) {
+                             uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_update<<<dim3(blocks, 1, count), 256, 0, st>>>(P, S, val, stride, i0, i1, atomic);
+    k_sn_update<<<dim3(blocks, 1, count), 256, 0, st>>>(P, S, val, stride, b0, atomic);
     return cudaGetLastError();
 }
 
-cudaError_t launch_sn_positions(const DevPattern &P, const SnPlanDev &S, const uint32_t *tgt_off, uint32_t nsn,
-                                uint32_t *pos, cudaStream_t st) {
+cudaError_t launch_sn_targets(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint4 *tgt, cudaStream_t st) {
     if (nsn == 0) return cudaSuccess;
-    k_sn_positions<<<148 * 16, 256, 0, st>>>(P, S, tgt_off, nsn, pos);
+    k_sn_targets<<<148 * 8, 256, 0, st>>>(P, S, nsn, tgt);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sn_positions(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint32_t *pos,
+                                cudaStream_t st) {
+    if (nsn == 0) return cudaSuccess;
+    k_sn_positions<<<148 * 16, 256, 0, st>>>(P, S, nsn, pos);
     return cudaGetLastError();
 }
 

@@ -42,30 +42,32 @@ cudaError_t launch_factor_chain(const DevPattern &P, const FactorPlanDev &F, flo
 constexpr uint32_t kSnMaxWidth = 64;       // widest supernode
 constexpr uint32_t kSnPanelThreads = 128;  // threads of a panel block (rows or targets per block)
 
-// Supernodes in level order: first column, width; block prefixes of the panel
-// and update launches; the update's position table (nullable) with its offset
-// per supernode.
+// Supernodes in level order: their records, the block maps of the panel and
+// update launches, the target metadata and the update's position table
+// (nullable) with its offset per supernode.
 struct SnPlanDev {
-    const uint32_t *sn_col;
-    const uint32_t *sn_w;
-    const uint32_t *pblk;      // [count + 1]
-    const uint32_t *ublk;      // [count + 1]
-    const uint32_t *pos;       // CSC positions of the update outputs, or nullptr
-    const uint64_t *pos_off;   // [count]
+    const uint4 *meta;        // per supernode: {first column, width, L21 rows m, targets nt}
+    const uint2 *pmap;        // per panel block: {supernode, part}
+    const uint2 *umap;        // per update block: {supernode, tile}
+    const uint32_t *tgt_off;  // [count + 1] prefix of the targets
+    const uint4 *tgt;         // per target: {CSC position of row l, rows present (0: none), extra rows, 0}
+    const uint32_t *pos;      // CSC positions of the update outputs, or nullptr
+    const uint64_t *pos_off;  // [count]
 };
 
-// Supernodes [i0, i1) of one level; blocks = pblk[i1] - pblk[i0] (panel) or
-// ublk[i1] - ublk[i0] (update).  diag runs before panel, panel before update.
+// Supernodes [i0, i1) of one level (diag); blocks [b0, b0 + blocks) of the
+// panel or update map.  diag runs before panel, panel before update.
 cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                            const float *pert_z, uint32_t i0, uint32_t i1, cudaStream_t st);
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                            const float *pert_z, uint32_t i0, uint32_t i1, uint32_t blocks, cudaStream_t st);
+                            const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st);
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                             uint32_t i0, uint32_t i1, uint32_t blocks, uint32_t atomic, cudaStream_t st);
-// Fills the position table (S.pos) of all nsn supernodes; tgt_off[nsn + 1] is
-// the prefix of their target counts.
-cudaError_t launch_sn_positions(const DevPattern &P, const SnPlanDev &S, const uint32_t *tgt_off, uint32_t nsn,
-                                uint32_t *pos, cudaStream_t st);
+                             uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st);
+// Setup, once per pattern: the target metadata (S.meta, S.tgt_off set), then
+// the position table (S.tgt set).
+cudaError_t launch_sn_targets(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint4 *tgt, cudaStream_t st);
+cudaError_t launch_sn_positions(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint32_t *pos,
+                                cudaStream_t st);
 
 // ------------------------------------------------------------- dense tail --
 // The trailing m x m block [t, n) x [t, n) is fully dense; element (i, j) of it
