@@ -178,7 +178,7 @@ struct glu_handle_s {
     DevBuf d_sn_meta, d_sn_pmap, d_sn_umap, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
-    DevBuf d_ss_map[2], d_ss_meta[2];  // supernodal L and U sweeps
+    DevBuf d_ss_map[2], d_ss_meta[2], d_ss_small[2];  // supernodal L and U sweeps
     std::vector<SnSweepLevel> ss_levels[2];
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
@@ -546,33 +546,44 @@ Status build_sn_plan(glu_handle_s *h) {
         }
         std::vector<uint4> smeta(ns);
         std::vector<uint2> smap;
+        std::vector<uint32_t> ssmall;
         h->ss_levels[u].clear();
         for (int32_t l = 0; l < snl; ++l) {
             const uint32_t b0 = uint32_t(smap.size());
+            const size_t small0 = ssmall.size();
             for (uint32_t i = lc[l]; i < lc[l + 1]; ++i) {
                 const uint32_t q = ord[i];
                 const uint32_t s0 = first[q], w = first[q + 1] - s0, last = first[q + 1] - 1;
-                uint64_t work;
+                uint64_t work, off;
                 if (!u) {
                     smeta[i] = make_uint4(s0, w, s.l_col_ptr[last] + 1, nl(last));
-                    work = (nl(last) + kSnSweepRows - 1) / kSnSweepRows;
+                    off = nl(last);
+                    work = (off + kSnSweepRows - 1) / kSnSweepRows;
                 } else {
-                    uint64_t above = 0;
-                    for (uint32_t c = s0; c <= last; ++c) above += (s.l_col_ptr[c] - (c - s0)) - s.sym_c_ptr[c];
+                    off = 0;
+                    for (uint32_t c = s0; c <= last; ++c) off += (s.l_col_ptr[c] - (c - s0)) - s.sym_c_ptr[c];
                     smeta[i] = make_uint4(s0, w, 0u, 0u);
-                    work = (above + kSnSweepAbove - 1) / kSnSweepAbove;
+                    work = (off + kSnSweepAbove - 1) / kSnSweepAbove;
+                }
+                if (w <= kSnSmallWidth && off <= 32) {
+                    ssmall.push_back(i);
+                    continue;
                 }
                 work = std::max<uint64_t>(work, 1);
                 if (smap.size() + work > UINT32_MAX) return set_error(GLU_ERR_UNSUPPORTED, "solve schedule too large");
                 for (uint64_t bb = 0; bb < work; ++bb) smap.push_back(make_uint2(i, uint32_t(bb)));
             }
+            for (size_t g = small0; g < ssmall.size(); g += 8)
+                smap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(8, ssmall.size() - g))));
             h->ss_levels[u].push_back(SnSweepLevel{b0, uint32_t(smap.size()) - b0});
         }
+        GLU_CUDA(upload(h->d_ss_small[u], ssmall), "upload solve plan");
         GLU_CUDA(upload(h->d_ss_map[u], smap), "upload solve plan");
         GLU_CUDA(upload(h->d_ss_meta[u], smeta), "upload solve plan");
         SnSweepPlan &pl = h->S.sn[u];
         pl.map = h->d_ss_map[u].as<uint2>();
         pl.meta = h->d_ss_meta[u].as<uint4>();
+        pl.small = h->d_ss_small[u].as<uint32_t>();
         pl.levels = h->ss_levels[u].data();
         pl.nlev = uint32_t(h->ss_levels[u].size());
         h->stats.sn_sweep_levels += pl.nlev;

@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
 // updates each entry from one thread: C is loaded, the K products are applied
 // in column order, C is stored.  Target positions come from the precomputed
 // table S.pos when present, else from a search in column j's rows.
-__global__ void __launch_bounds__(256, 3) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
+__global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
                                                       uint32_t b0, uint32_t atomic) {
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
     __shared__ __align__(16) float sU[kSnMaxWidth][kTLd];

@@ -145,11 +145,14 @@ struct SnSweepLevel {
     uint32_t b0, blocks;  // first block, blocks
 };
 struct SnSweepPlan {
-    const uint2 *map = nullptr;
+    const uint2 *map = nullptr;     // {supernode, part} or {first of small[], kSnSmallFlag | count}
     const uint4 *meta = nullptr;
+    const uint32_t *small = nullptr;  // small supernodes, grouped eight to a block
     const SnSweepLevel *levels = nullptr;  // host array
     uint32_t nlev = 0;
 };
+constexpr uint32_t kSnSmallWidth = 16;         // small supernode: width <= this, <= 32 off-diagonal rows/entries
+constexpr uint32_t kSnSmallFlag = 0x80000000u;
 constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep
 constexpr uint32_t kSnSweepAbove = 1024;  // U entries per block of the U sweep
 

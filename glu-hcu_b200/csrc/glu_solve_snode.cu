@@ -14,7 +14,9 @@
 // for the supernodes whose L21 rows fall in it; U — for the supernodes that
 // hold its update targets.  Finished unknowns go to xo (another block of the
 // same supernode may still read y_S) and are copied back after the sweep.
-// Every block finds its supernode and part through a precomputed map.
+// Every block finds its supernode and part through a precomputed map; small
+// supernodes (width <= kSnSmallWidth with at most 32 off-diagonal rows or
+// entries) go eight to a block, one warp each.
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 
@@ -22,13 +24,108 @@ namespace glu {
 
 namespace {
 constexpr int kLD = kSnMaxWidth + 1;
+constexpr uint32_t kFull = 0xffffffffu;
+
+// L sweep of one small supernode (w <= kSnSmallWidth, m <= 32) by one warp:
+// lane k holds unknown s+k and L21 row k; the entries it needs are loaded
+// before the dependency chain starts.
+__device__ __forceinline__ void sn_sweep_l_small(const DevPattern &P, const SnSweepPlan &W,
+                                                 const float *__restrict__ val, float *y, float *xo, uint32_t nrhs,
+                                                 uint32_t i, uint32_t lane) {
+    constexpr int SW = int(kSnSmallWidth);
+    const uint4 md = W.meta[i];
+    const uint32_t s = md.x, w = md.y, lbase = md.z, m = md.w, l = s + w - 1, n = P.n;
+    const uint32_t dl = lane < w ? P.diag[s + lane] : 0u;
+    float lrow[SW], l21[SW];
+#pragma unroll
+    for (int c = 0; c < SW; ++c) {
+        const uint32_t dc = __shfl_sync(kFull, dl, c);
+        lrow[c] = (uint32_t(c) < lane && lane < w) ? __ldg(val + dc + (lane - c)) : 0.0f;
+        l21[c] = (lane < m && uint32_t(c) < w) ? __ldg(val + dc + (l + 1 - (s + c)) + lane) : 0.0f;
+    }
+    const uint32_t target = lane < m ? __ldg(P.ridx + lbase + lane) : 0u;
+    for (uint32_t q = 0; q < nrhs; ++q) {
+        float *yq = y + size_t(q) * n;
+        float v = lane < w ? __ldcg(yq + s + lane) : 0.0f;
+#pragma unroll
+        for (int c = 0; c + 1 < SW; ++c) {
+            if (uint32_t(c) + 1 >= w) break;
+            const float xc = __shfl_sync(kFull, v, c);
+            if (lane > uint32_t(c) && lane < w) v = __fsub_rn(v, __fmul_rn(lrow[c], xc));
+        }
+        if (lane < w) xo[size_t(q) * n + s + lane] = v;
+        float acc = 0.0f;
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+            if (uint32_t(c) >= w) break;
+            acc = fmaf(l21[c], __shfl_sync(kFull, v, c), acc);
+        }
+        if (lane < m && acc != 0.0f) atomicAdd(yq + target, -acc);
+    }
 }
 
-__global__ void __launch_bounds__(256) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+// U sweep of one small supernode (w <= kSnSmallWidth, at most 32 entries above
+// the block) by one warp: lane k holds unknown s+k and above-block entry k.
+__device__ __forceinline__ void sn_sweep_u_small(const DevPattern &P, const SnSweepPlan &W,
+                                                 const float *__restrict__ val, float *y, float *xo, uint32_t nrhs,
+                                                 uint32_t i, uint32_t lane) {
+    constexpr int SW = int(kSnSmallWidth);
+    const uint4 md = W.meta[i];
+    const uint32_t s = md.x, w = md.y, n = P.n;
+    const uint32_t dl = lane < w ? P.diag[s + lane] : 0u;
+    const uint32_t cp = lane < w ? P.cptr[s + lane] : 0u;
+    const uint32_t cnt = lane < w ? (dl - lane) - cp : 0u;  // entries of column s+lane above the block
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= uint32_t(o)) incl += v;
+    }
+    const uint32_t pre = incl - cnt, total = __shfl_sync(kFull, incl, 31);
+    uint32_t col = 0;  // column of entry `lane`: the last c < w with pre_c <= lane
+#pragma unroll
+    for (int c = 1; c < SW; ++c) {
+        const uint32_t pc = __shfl_sync(kFull, pre, c);
+        if (uint32_t(c) < w && pc <= lane) col = c;
+    }
+    const uint32_t pcol = __shfl_sync(kFull, cp, col) + (lane - __shfl_sync(kFull, pre, col));
+    const bool ev = lane < total;
+    const uint32_t tg = ev ? __ldg(P.ridx + pcol) : 0u;
+    const float ue = ev ? __ldg(val + pcol) : 0.0f;
+    float urow[SW];  // U(s+lane, s+cc) for cc > lane, at diag[s+cc] - (cc - lane)
+#pragma unroll
+    for (int cc = 0; cc < SW; ++cc) {
+        const uint32_t dcc = __shfl_sync(kFull, dl, cc);
+        urow[cc] = (lane < uint32_t(cc) && uint32_t(cc) < w) ? __ldg(val + dcc - (cc - lane)) : 0.0f;
+    }
+    const float piv = lane < w ? __ldg(val + dl) : 1.0f;
+    for (uint32_t q = 0; q < nrhs; ++q) {
+        float *yq = y + size_t(q) * n;
+        float v = lane < w ? __ldcg(yq + s + lane) : 0.0f;
+#pragma unroll
+        for (int cc = SW - 1; cc >= 0; --cc) {
+            if (uint32_t(cc) >= w) continue;
+            const float xc = __shfl_sync(kFull, v, cc) / __shfl_sync(kFull, piv, cc);
+            if (lane == uint32_t(cc)) v = xc;
+            if (lane < uint32_t(cc)) v = __fsub_rn(v, __fmul_rn(urow[cc], xc));
+        }
+        if (lane < w) xo[size_t(q) * n + s + lane] = v;
+        const float xe = __shfl_sync(kFull, v, col);
+        if (ev && xe != 0.0f) atomicAdd(yq + tg, -__fmul_rn(ue, xe));
+    }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0) {
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     const uint2 bi = W.map[b0 + blockIdx.x];
+    if (bi.y & kSnSmallFlag) {  // a group of small supernodes, one per warp
+        const uint32_t wi = threadIdx.x >> 5;
+        if (wi < (bi.y & ~kSnSmallFlag)) sn_sweep_l_small(P, W, val, y, xo, nrhs, W.small[bi.x + wi], threadIdx.x & 31);
+        return;
+    }
     const uint4 md = W.meta[bi.x];
     const uint32_t s = md.x, w = md.y, lbase = md.z, m = md.w, t = bi.y;
     const uint32_t l = s + w - 1;
@@ -68,12 +165,17 @@ __global__ void __launch_bounds__(256) k_sn_sweep_l(DevPattern P, SnSweepPlan W,
     }
 }
 
-__global__ void __launch_bounds__(256) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+__global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0) {
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     __shared__ uint32_t pre[kSnMaxWidth + 1];
     const uint2 bi = W.map[b0 + blockIdx.x];
+    if (bi.y & kSnSmallFlag) {  // a group of small supernodes, one per warp
+        const uint32_t wi = threadIdx.x >> 5;
+        if (wi < (bi.y & ~kSnSmallFlag)) sn_sweep_u_small(P, W, val, y, xo, nrhs, W.small[bi.x + wi], threadIdx.x & 31);
+        return;
+    }
     const uint32_t s = W.meta[bi.x].x, w = W.meta[bi.x].y, t = bi.y;
     const uint32_t tid = threadIdx.x, n = P.n;
     // U11 with its diagonal: U(s+k, s+c), k <= c, at diag[s+c] - (c - k)
