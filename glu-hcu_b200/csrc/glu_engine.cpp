@@ -175,7 +175,7 @@ struct glu_handle_s {
     // supernodal plan of the sparse part (used when tune.sn_width != 0)
     bool use_sn = false;
     uint32_t nsn = 0;
-    DevBuf d_sn_meta, d_sn_pmap, d_sn_umap, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
+    DevBuf d_sn_meta, d_sn_pmap, d_sn_umap, d_sn_psmall, d_sn_usmall, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
     DevBuf d_ss_map[2], d_ss_meta[2], d_ss_small[2];  // supernodal L and U sweeps
@@ -456,13 +456,14 @@ Status build_sn_plan(glu_handle_s *h) {
     }
     std::vector<uint4> meta(ns);
     std::vector<uint2> pmap, umap;
-    std::vector<uint32_t> tgt(size_t(ns) + 1, 0);
+    std::vector<uint32_t> psmall, usmall, tgt(size_t(ns) + 1, 0);
     std::vector<uint64_t> pos_off(size_t(ns) + 1, 0);
     const uint32_t PT = kSnPanelThreads, UT = 64, TW = kSnPanelThreads / 32;
     double upd_flops = 0, upd_bytes = 0, pan_bytes = 0;
     for (int32_t l = 0; l < nlev; ++l) {
         uint32_t updating = 0, wide = 0;
         const uint32_t pb0 = uint32_t(pmap.size()), ub0 = uint32_t(umap.size());
+        const size_t ps0 = psmall.size(), us0 = usmall.size();
         for (uint32_t i = lcount[l]; i < lcount[l + 1]; ++i) {
             const uint32_t q = order[i];
             const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
@@ -475,14 +476,27 @@ Status build_sn_plan(glu_handle_s *h) {
             if (pmap.size() + pb > UINT32_MAX || umap.size() + tiles > UINT32_MAX ||
                 uint64_t(tgt[i]) + nt > UINT32_MAX)
                 return set_error(GLU_ERR_UNSUPPORTED, "supernodal schedule too large");
-            for (uint64_t bb = 0; bb < pb; ++bb) pmap.push_back(make_uint2(i, uint32_t(bb)));
-            for (uint64_t bb = 0; bb < tiles; ++bb) umap.push_back(make_uint2(i, uint32_t(bb)));
+            // small supernodes: one warp each, grouped four (panel) or eight (update) to a block
+            const bool small = h->tune.sn_small && w <= kSnSmallWidth && m <= 32 && nt <= 32;
+            if (pb && small)
+                psmall.push_back(i);
+            else
+                for (uint64_t bb = 0; bb < pb; ++bb) pmap.push_back(make_uint2(i, uint32_t(bb)));
+            if (tiles && small && m * nt <= 256)
+                usmall.push_back(i);
+            else
+                for (uint64_t bb = 0; bb < tiles; ++bb) umap.push_back(make_uint2(i, uint32_t(bb)));
             tgt[i + 1] = tgt[i] + uint32_t(nt);
             pos_off[i + 1] = pos_off[i] + m * nt;
             upd_flops += 2.0 * double(m) * w * nt;
             upd_bytes += 4.0 * (double(m) * w + double(w) * nt) + 8.0 * double(m) * nt;
             pan_bytes += 8.0 * (double(m) * w + double(w) * nt) + (w >= 2 ? 8.0 * w * w : 0.0);
         }
+        for (size_t g = ps0; g < psmall.size(); g += kSnPanelThreads / 32)
+            pmap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(kSnPanelThreads / 32,
+                                                                                             psmall.size() - g))));
+        for (size_t g = us0; g < usmall.size(); g += 8)
+            umap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(8, usmall.size() - g))));
         const uint32_t i0 = lcount[l], i1 = lcount[l + 1];
         h->sn_levels.push_back(SnLevel{i0, i1, pb0, uint32_t(pmap.size()) - pb0, ub0, uint32_t(umap.size()) - ub0,
                                        updating > 1 ? 1u : 0u, wide ? 1u : 0u});
@@ -491,12 +505,14 @@ Status build_sn_plan(glu_handle_s *h) {
     GLU_CUDA(upload(h->d_sn_meta, meta), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pmap, pmap), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_umap, umap), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_psmall, psmall), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_usmall, usmall), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_tgt_off, tgt), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pos_off, pos_off), "upload supernodes");
     GLU_CUDA(h->d_sn_tgt.alloc(sizeof(uint4) * std::max<uint32_t>(tgt[ns], 1)), "allocate supernode targets");
-    h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),    h->d_sn_pmap.as<uint2>(), h->d_sn_umap.as<uint2>(),
-                      h->d_sn_tgt_off.as<uint32_t>(), h->d_sn_tgt.as<uint4>(), nullptr,
-                      h->d_sn_pos_off.as<uint64_t>()};
+    h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),      h->d_sn_pmap.as<uint2>(),  h->d_sn_umap.as<uint2>(),
+                      h->d_sn_psmall.as<uint32_t>(), h->d_sn_usmall.as<uint32_t>(), h->d_sn_tgt_off.as<uint32_t>(),
+                      h->d_sn_tgt.as<uint4>(),       nullptr,                    h->d_sn_pos_off.as<uint64_t>()};
     GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
     GLU_CUDA(cudaDeviceSynchronize(), "supernode targets");
     // position table of the update scatter, when it fits in a quarter of the free memory
@@ -565,7 +581,7 @@ Status build_sn_plan(glu_handle_s *h) {
                     smeta[i] = make_uint4(s0, w, 0u, 0u);
                     work = (off + kSnSweepAbove - 1) / kSnSweepAbove;
                 }
-                if (w <= kSnSmallWidth && off <= 32) {
+                if (h->tune.sn_small && w <= kSnSmallWidth && off <= 32) {
                     ssmall.push_back(i);
                     continue;
                 }
@@ -792,7 +808,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");

@@ -158,6 +158,119 @@ __device__ __forceinline__ void sn_u12_warp(float *__restrict__ val, const Sn &d
     if (p1) st_cg(val + pl - (w - 1 - k1), a1);
 }
 
+constexpr uint32_t kFull = 0xffffffffu;
+
+// Panel of one small supernode (w <= kSnSmallWidth, m <= 32, nt <= 32) by one
+// warp: lane r solves L21 row r, lane j solves target column j of U12, with
+// the factored diagonal block read in place (broadcast loads).
+__device__ __forceinline__ void sn_panel_small(const DevPattern &P, const SnPlanDev &S, float *__restrict__ val,
+                                               uint32_t i, float pert, uint32_t lane) {
+    constexpr int SW = int(kSnSmallWidth);
+    const Sn d = sn_load(S, i);
+    const uint32_t w = d.w;
+    if (w == 1) {
+        // numeric.cu:133-143: pivot (perturbed when the column has an L part), L /= pivot
+        const uint32_t dk = P.diag[d.s];
+        const float p = ld_cg(val + dk);
+        const float de = (pert > 0.0f && fabsf(p) < pert) ? pert : p;  // m > 0 here
+        if (lane < d.m) st_cg(val + dk + 1 + lane, ld_cg(val + dk + 1 + lane) / de);
+        if (lane == 0 && de != p) st_cg(val + dk, de);
+        return;
+    }
+    const uint32_t dl = lane < w ? P.diag[d.s + lane] : 0u;  // position of the diagonal of column s+lane
+    // row `lane` of L21: x U11 = a
+    {
+        const bool rv = lane < d.m;
+        float a[SW];
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+            const uint32_t dc = __shfl_sync(kFull, dl, c);
+            a[c] = (rv && uint32_t(c) < w) ? ld_cg(val + dc + (d.l + 1 - (d.s + c)) + lane) : 0.0f;
+        }
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+            if (uint32_t(c) >= w) break;
+            const float l = a[c] / ld_cg(val + __shfl_sync(kFull, dl, c));
+            a[c] = l;
+#pragma unroll
+            for (int j = c + 1; j < SW; ++j) {
+                const uint32_t dj = __shfl_sync(kFull, dl, j);
+                if (uint32_t(j) < w) a[j] = fmaf(-l, ld_cg(val + dj - (j - c)), a[j]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+            const uint32_t dc = __shfl_sync(kFull, dl, c);  // every lane takes part in the shuffle
+            if (rv && uint32_t(c) < w) st_cg(val + dc + (d.l + 1 - (d.s + c)) + lane, a[c]);
+        }
+    }
+    // target column `lane` of U12: L11 x = a over the rows present
+    {
+        uint4 g = make_uint4(0u, 0u, 0u, 0u);
+        if (lane < d.nt) g = S.tgt[S.tgt_off[i] + lane];
+        const uint32_t z = w - g.y;  // g.y == 0: no target (z = w, nothing loaded or stored)
+        float a[SW];
+#pragma unroll
+        for (int k = 0; k < SW; ++k) a[k] = (uint32_t(k) < w && uint32_t(k) >= z) ? ld_cg(val + g.x - (w - 1 - k)) : 0.0f;
+#pragma unroll
+        for (int r = 0; r < SW; ++r) {
+            if (uint32_t(r) >= w) break;
+            const uint32_t dr = __shfl_sync(kFull, dl, r);
+            if (uint32_t(r) >= z) {
+                const float u = a[r];
+#pragma unroll
+                for (int k = r + 1; k < SW; ++k)
+                    if (uint32_t(k) < w) a[k] = fmaf(-ld_cg(val + dr + (k - r)), u, a[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < SW; ++k)
+            if (uint32_t(k) < w && uint32_t(k) >= z) st_cg(val + g.x - (w - 1 - k), a[k]);
+    }
+}
+
+// Update of one small supernode (w <= kSnSmallWidth, m * nt <= 256) by one
+// warp, its m x nt outputs 32 at a time (same arithmetic as the tiles).
+__device__ __forceinline__ void sn_update_small(const DevPattern &P, const SnPlanDev &S, float *__restrict__ val,
+                                                uint32_t i, bool atomic, uint32_t lane) {
+    constexpr int SW = int(kSnSmallWidth);
+    const Sn d = sn_load(S, i);
+    const uint32_t w = d.w, m = d.m, nout = d.m * d.nt;
+    // L21 base of column s+lane: L21(r, c) at diag[s+c] + (l + 1 - (s+c)) + r
+    const uint32_t bl = lane < w ? P.diag[d.s + lane] + (d.l + 1 - (d.s + lane)) : 0u;
+    const uint32_t g0 = S.tgt_off[i];
+    const uint32_t lbase = P.diag[d.l] + 1;
+    for (uint32_t o0 = 0; o0 < nout; o0 += 32) {
+        const uint32_t o = o0 + lane;
+        const bool ov = o < nout;
+        const uint32_t jt = ov ? o / m : 0u, r = ov ? o - jt * m : 0u;
+        uint4 g = make_uint4(0u, 0u, 0u, 0u);
+        if (ov) g = S.tgt[g0 + jt];
+        const bool v = ov && g.y != 0;
+        uint32_t q = g.x + 1 + r;
+        if (v && g.z)
+            q = S.pos ? __ldg(S.pos + S.pos_off[i] + uint64_t(jt) * m + r)
+                      : lower_bound_u32(P.ridx, q, q + g.z + 1, __ldg(P.ridx + lbase + r));
+        float acc = (v && !atomic) ? ld_cg(val + q) : 0.0f;
+#pragma unroll
+        for (int c = 0; c < SW; ++c) {
+            if (uint32_t(c) >= w) break;
+            const uint32_t bc = __shfl_sync(kFull, bl, c);
+            if (v) {
+                const float lv = ld_cg(val + bc + r);
+                const float uv = (uint32_t(c) + g.y >= w) ? ld_cg(val + g.x - (w - 1 - c)) : 0.0f;
+                acc = atomic ? fmaf(lv, uv, acc) : fmaf(-lv, uv, acc);
+            }
+        }
+        if (v) {
+            if (atomic)
+                atomicAdd(val + q, -acc);
+            else
+                st_cg(val + q, acc);
+        }
+    }
+}
+
 }  // namespace
 
 // Diagonal blocks of one level's supernodes [i0, i0 + gridDim.x), factored in
@@ -185,6 +298,11 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
     const uint2 bi = S.pmap[b0 + blockIdx.x];
+    if (bi.y & kSnSmallFlag) {  // small supernodes, one per warp
+        const uint32_t wi = threadIdx.x >> 5;
+        if (wi < (bi.y & ~kSnSmallFlag)) sn_panel_small(P, S, val, S.psmall[bi.x + wi], pert, threadIdx.x & 31);
+        return;
+    }
     const uint32_t i = bi.x, t = bi.y;
     const Sn d = sn_load(S, i);
     const uint32_t tid = threadIdx.x;
@@ -258,6 +376,11 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
     __shared__ uint32_t sPl[kTile], sLen[kTile], sEx[kTile];
     float *val = val_base + blockIdx.z * stride;
     const uint2 bi = S.umap[b0 + blockIdx.x];
+    if (bi.y & kSnSmallFlag) {  // small supernodes, one per warp
+        const uint32_t wi = threadIdx.x >> 5;
+        if (wi < (bi.y & ~kSnSmallFlag)) sn_update_small(P, S, val, S.usmall[bi.x + wi], atomic != 0, threadIdx.x & 31);
+        return;
+    }
     const uint32_t i = bi.x, t = bi.y;
     const Sn d = sn_load(S, i);
     const uint32_t tid = threadIdx.x;

@@ -42,13 +42,18 @@ cudaError_t launch_factor_chain(const DevPattern &P, const FactorPlanDev &F, flo
 constexpr uint32_t kSnMaxWidth = 64;       // widest supernode
 constexpr uint32_t kSnPanelThreads = 128;  // threads of a panel block (rows or targets per block)
 
+constexpr uint32_t kSnSmallWidth = 16;         // small supernode: width <= this, few off-diagonal rows/entries
+constexpr uint32_t kSnSmallFlag = 0x80000000u;  // block-map entry of a group of small supernodes
+
 // Supernodes in level order: their records, the block maps of the panel and
 // update launches, the target metadata and the update's position table
 // (nullable) with its offset per supernode.
 struct SnPlanDev {
     const uint4 *meta;        // per supernode: {first column, width, L21 rows m, targets nt}
-    const uint2 *pmap;        // per panel block: {supernode, part}
-    const uint2 *umap;        // per update block: {supernode, tile}
+    const uint2 *pmap;        // per panel block: {supernode, part} or {first of psmall, kSnSmallFlag | count}
+    const uint2 *umap;        // per update block: {supernode, tile} or {first of usmall, kSnSmallFlag | count}
+    const uint32_t *psmall;   // small supernodes of the panel launches, four to a block
+    const uint32_t *usmall;   // small supernodes of the update launches, eight to a block
     const uint32_t *tgt_off;  // [count + 1] prefix of the targets
     const uint4 *tgt;         // per target: {CSC position of row l, rows present (0: none), extra rows, 0}
     const uint32_t *pos;      // CSC positions of the update outputs, or nullptr
@@ -151,8 +156,6 @@ struct SnSweepPlan {
     const SnSweepLevel *levels = nullptr;  // host array
     uint32_t nlev = 0;
 };
-constexpr uint32_t kSnSmallWidth = 16;         // small supernode: width <= this, <= 32 off-diagonal rows/entries
-constexpr uint32_t kSnSmallFlag = 0x80000000u;
 constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep
 constexpr uint32_t kSnSweepAbove = 1024;  // U entries per block of the U sweep
 

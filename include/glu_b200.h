@@ -228,6 +228,8 @@ typedef struct {
     uint32_t solve_cluster;    /* CTAs of that cluster (1..16)                   */
     uint32_t sn_width;         /* widest supernode of the sparse factorization
                                   (1..64); 0 factors column by column            */
+    uint32_t sn_small;         /* 1: supernodes with few rows and targets run one
+                                  per warp, grouped into blocks; 0: a block each */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

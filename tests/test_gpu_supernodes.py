@@ -116,3 +116,16 @@ def test_supernodes_refined_solve():
     x = lu.solve(b, refine=True, tol=1e-12, maxiter=30)
     M = sp.csc_matrix(A[:3], shape=(n, n))
     assert np.linalg.norm(M @ x - b) / np.linalg.norm(b) <= 1e-10
+
+
+@pytest.mark.parametrize("small", [0, 1])
+@pytest.mark.parametrize("width", [3, 4])
+def test_small_supernode_grouping_matches_oracle(small, width):
+    """Supernodes with few rows and targets run one per warp (sn_small = 1) or a
+    block each (0); both must match the oracle, including the last pivots of a
+    dense trailing region cut into narrow supernodes."""
+    A = _matrix("nodal2500")
+    lu = _factor(A, sn_width=width, dense_tail_min=NO_TAIL, sn_small=small)
+    ref, p = _reference(lu)
+    err = col_max_rel(lu.lu_values(), ref, p["sym_c_ptr"])
+    assert err <= FACTOR_TOL, (small, width, err)
