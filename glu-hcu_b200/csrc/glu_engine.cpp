@@ -200,6 +200,10 @@ struct glu_handle_s {
     double *h_norms = nullptr;     // pinned
     size_t h_norms_cap = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // dense tail look-ahead: high-priority stream for the panels, fork /
+    // panel-done / rest-done events
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_panel = nullptr, ev_rest = nullptr;
     KernelProfiler prof;
     bool factored = false;
     glu_stats stats{};
@@ -209,6 +213,10 @@ struct glu_handle_s {
         if (h_norms) cudaFreeHost(h_norms);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_panel) cudaEventDestroy(ev_panel);
+        if (ev_rest) cudaEventDestroy(ev_rest);
+        if (aux) cudaStreamDestroy(aux);
     }
 };
 
@@ -267,6 +275,8 @@ void find_full_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t
 // an active column < t.  Returns the t of least estimated time with
 // m <= max_m (t = n: no dense tail).
 constexpr double kDenseRate = 30e12, kPanelLatency = 20e-6;
+// Default width from which trailing blocks factor with panel look-ahead.
+constexpr uint32_t kLookaheadMin = 3072;
 constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
 
 uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
@@ -808,7 +818,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -832,6 +842,14 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_status), 256), "allocate pinned");
     GLU_CUDA(cudaEventCreate(&h->ev0), "event");
     GLU_CUDA(cudaEventCreate(&h->ev1), "event");
+    {
+        int least = 0, greatest = 0;
+        GLU_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+        GLU_CUDA(cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, greatest), "stream");
+    }
+    GLU_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming), "event");
+    GLU_CUDA(cudaEventCreateWithFlags(&h->ev_panel, cudaEventDisableTiming), "event");
+    GLU_CUDA(cudaEventCreateWithFlags(&h->ev_rest, cudaEventDisableTiming), "event");
 
     // level sets on the device
     {
@@ -1316,17 +1334,68 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         GLU_LAUNCH(KK_DGATHER,
                    launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
                    "factor (dense gather)");
-    for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
-        uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
-        uint32_t last_has_l = 0;  // the last column of the matrix has no L part
-        GLU_LAUNCH(KK_PANEL,
-                   launch_dense_panel(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb, pert,
-                                      h->d_diag_scratch.as<float>(), last_has_l, st),
-                   "factor (dense panel)");
-        GLU_LAUNCH(KK_UPDATE,
-                   launch_dense_update(dbase, dstride, count, h->d_doff.as<uint32_t>(), h->m, k0, kb,
-                                       h->d_diag_scratch.as<float>(), st),
-                   "factor (dense update)");
+    // Look-ahead (trailing blocks of tune.dense_lookahead columns or more): the panels
+    // and, after the panel at k0, the next panel's row and column strips of the
+    // trailing update run on a high-priority internal stream; the rest of the
+    // update runs on st, concurrently with the next panel, which it does not
+    // touch.  The strips of step p+1 wait for the rest of step p (the same
+    // entries, updated in step order).
+    const bool lookahead = h->aux && h->tune.dense_lookahead && h->m >= h->tune.dense_lookahead && h->m > kDenseNB;
+    const uint32_t *doff = h->d_doff.as<uint32_t>();
+    float *dscr = h->d_diag_scratch.as<float>();
+    if (!lookahead) {
+        for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
+            const uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
+            const uint32_t rest = h->m - (k0 + kb);
+            GLU_LAUNCH(KK_PANEL, launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, st),
+                       "factor (dense panel)");
+            GLU_LAUNCH(KK_UPDATE,
+                       launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
+                                           DenseRegion{0, rest, 0, rest, 1}, st),
+                       "factor (dense update)");
+        }
+    } else {
+        cudaStream_t hp = h->aux;
+        GLU_CUDA(cudaEventRecord(h->ev_fork, st), "event");
+        GLU_CUDA(cudaStreamWaitEvent(hp, h->ev_fork, 0), "stream wait");
+        bool rest_pending = false;
+        const uint32_t nb = kDenseNB;
+        for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
+            const uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
+            const uint32_t rest = h->m - (k0 + kb);
+            GLU_CUDA(pf.begin(hp), "profile event");
+            GLU_CUDA(launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, hp),
+                     "factor (dense panel)");
+            GLU_CUDA(pf.end(KK_PANEL, hp), "profile event");
+            if (rest_pending) GLU_CUDA(cudaStreamWaitEvent(hp, h->ev_rest, 0), "stream wait");
+            if (rest <= nb) {  // last steps: the whole update after the panel
+                GLU_CUDA(pf.begin(hp), "profile event");
+                GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
+                                             DenseRegion{0, rest, 0, rest, 1}, hp),
+                         "factor (dense update)");
+                GLU_CUDA(pf.end(KK_UPDATE, hp), "profile event");
+                rest_pending = false;
+                continue;
+            }
+            GLU_CUDA(cudaEventRecord(h->ev_panel, hp), "event");
+            GLU_CUDA(pf.begin(hp), "profile event");
+            GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, DenseRegion{0, nb, 0, rest, 1},
+                                         hp),
+                     "factor (dense update)");
+            GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
+                                         DenseRegion{nb, rest, 0, nb, 0}, hp),
+                     "factor (dense update)");
+            GLU_CUDA(pf.end(KK_UPDATE, hp), "profile event");
+            GLU_CUDA(cudaStreamWaitEvent(st, h->ev_panel, 0), "stream wait");
+            GLU_LAUNCH(KK_UPDATE,
+                       launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
+                                           DenseRegion{nb, rest, nb, rest, 0}, st),
+                       "factor (dense update)");
+            GLU_CUDA(cudaEventRecord(h->ev_rest, st), "event");
+            rest_pending = true;
+        }
+        GLU_CUDA(cudaEventRecord(h->ev_fork, hp), "event");
+        GLU_CUDA(cudaStreamWaitEvent(st, h->ev_fork, 0), "stream wait");
     }
     if (h->m && h->dense_buffer)
         GLU_LAUNCH(KK_DSCATTER,

@@ -248,7 +248,7 @@ template <int TB>
 __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64_t stride,
                                                          const uint32_t *__restrict__ doff,
                                                          uint32_t m, uint32_t k0, uint32_t kb,
-                                                         const float *diag_scratch) {
+                                                         const float *diag_scratch, DenseRegion reg) {
     constexpr int RM = UpdateTile<TB>::RM;
     constexpr int LDB = UpdateTile<TB>::LDB;
     constexpr int LDC = UpdateTile<TB>::LDC;
@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     float *sC = smem;                    // [col][row], padded (reuses sA/sB)
     float *val = val_base + blockIdx.z * stride;
     const uint32_t tid = threadIdx.x;
-    if (blockIdx.x == 0 && blockIdx.y == 0) {
+    if (reg.writeback && blockIdx.x == 0 && blockIdx.y == 0) {
         const float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
         for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
             uint32_t c = e / kb, r = e - c * kb;
@@ -268,9 +268,11 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     }
     const uint32_t r0 = k0 + kb;
     if (r0 >= m) return;
-    const uint32_t mp = m - r0;
-    const uint32_t rbase = blockIdx.x * TB, cbase = blockIdx.y * TB;
-    if (rbase >= mp || cbase >= mp) return;
+    // tile of the trailing block: rows [rbase, rbase + TB) of [r_lo, r_hi),
+    // columns [cbase, cbase + TB) of [c_lo, c_hi)
+    const uint32_t rbase = reg.r_lo + blockIdx.x * TB, cbase = reg.c_lo + blockIdx.y * TB;
+    const uint32_t rlim = reg.r_hi, mp = reg.c_hi;  // (mp: column limit)
+    if (rbase >= rlim || cbase >= mp) return;
     const uint32_t tx = tid & 15, ty = tid >> 4;
     // C tile into registers (through shared memory for coalescing): every
     // entry then receives its updates one k at a time, in increasing k, as in
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     for (uint32_t e = tid; e < uint32_t(TB) * TB; e += 256) {
         uint32_t col = e / TB, row = e - col * TB;
         float v = 0.0f;
-        if (cbase + col < mp && rbase + row < mp) v = ld_cg(val + doff[r0 + cbase + col] + r0 + rbase + row);
+        if (cbase + col < mp && rbase + row < rlim) v = ld_cg(val + doff[r0 + cbase + col] + r0 + rbase + row);
         sC[col * LDC + row] = v;
     }
     __syncthreads();
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     for (uint32_t e = tid; e < uint32_t(kDenseNB) * TB; e += 256) {
         uint32_t k = e / TB, row = e - k * TB;
         float v = 0.0f;
-        if (k < kb && rbase + row < mp) v = ld_cg(val + doff[k0 + k] + r0 + rbase + row);
+        if (k < kb && rbase + row < rlim) v = ld_cg(val + doff[k0 + k] + r0 + rbase + row);
         sA[k * TB + row] = v;
     }
     // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
 #pragma unroll 4
     for (uint32_t e = tid; e < uint32_t(TB) * TB; e += 256) {
         uint32_t col = e / TB, row = e - col * TB;
-        if (cbase + col < mp && rbase + row < mp)
+        if (cbase + col < mp && rbase + row < rlim)
             st_cg(val + doff[r0 + cbase + col] + r0 + rbase + row, sC[col * LDC + row]);
     }
 }
@@ -366,7 +368,7 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
 
 cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
-                                cudaStream_t st) {
+                                DenseRegion reg, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k_dense_update<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -377,16 +379,16 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
         if (e != cudaSuccess) return e;
         attr = true;
     }
-    const uint32_t rest = m - (k0 + kb);
-    const uint32_t t128 = (rest + 127) / 128;
-    if (uint64_t(t128) * t128 * count >= 2 * 148) {
-        dim3 grid(t128, t128, count);
-        k_dense_update<128><<<grid, 256, UpdateTile<128>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+    const uint32_t rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
+    const uint32_t cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
+    if ((rows == 0 || cols == 0) && !reg.writeback) return cudaSuccess;
+    const uint32_t r128 = (rows + 127) / 128, c128 = (cols + 127) / 128;
+    if (uint64_t(r128) * c128 * count >= 2 * 148) {
+        dim3 grid(r128, c128, count);
+        k_dense_update<128><<<grid, 256, UpdateTile<128>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch, reg);
     } else {
-        uint32_t t64 = (rest + 63) / 64;
-        if (t64 == 0) t64 = 1;
-        dim3 grid(t64, t64, count);
-        k_dense_update<64><<<grid, 256, UpdateTile<64>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch);
+        dim3 grid(std::max<uint32_t>((rows + 63) / 64, 1), std::max<uint32_t>((cols + 63) / 64, 1), count);
+        k_dense_update<64><<<grid, 256, UpdateTile<64>::Smem, st>>>(val, stride, doff, m, k0, kb, diag_scratch, reg);
     }
     return cudaGetLastError();
 }

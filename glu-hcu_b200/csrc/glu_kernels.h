@@ -84,9 +84,15 @@ constexpr int kGemmTile = 128;      // trailing-update tile
 cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
                                float *diag_scratch, uint32_t last_has_l, cudaStream_t st);
+// Part of the trailing update after the panel at k0: rows [r_lo, r_hi) and
+// columns [c_lo, c_hi) of the trailing block (relative to k0 + kb); writeback
+// != 0 also stores the factored diagonal block from diag_scratch.
+struct DenseRegion {
+    uint32_t r_lo, r_hi, c_lo, c_hi, writeback;
+};
 cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
-                                cudaStream_t st);
+                                DenseRegion reg, cudaStream_t st);
 // A trailing block that is dense but not completely filled is factored in a
 // separate m x m column-major buffer: gather copies the block's pattern
 // entries of the CSC values into the (zeroed) buffer, scatter copies the

@@ -230,6 +230,9 @@ typedef struct {
                                   (1..64); 0 factors column by column            */
     uint32_t sn_small;         /* 1: supernodes with few rows and targets run one
                                   per warp, grouped into blocks; 0: a block each */
+    uint32_t dense_lookahead;  /* dense trailing blocks at least this wide factor
+                                  the next panel during the current update
+                                  (0: never)                                     */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

@@ -129,3 +129,24 @@ def test_small_supernode_grouping_matches_oracle(small, width):
     ref, p = _reference(lu)
     err = col_max_rel(lu.lu_values(), ref, p["sym_c_ptr"])
     assert err <= FACTOR_TOL, (small, width, err)
+
+
+@pytest.mark.parametrize("name", ["config0", "mesh90"])
+def test_dense_lookahead_matches_oracle(name):
+    """The dense trailing block with the next panel factored during the
+    current update (forced on these small tails) against the oracle, and the
+    refined solve."""
+    import scipy.sparse as sp
+    from pyglu import synth
+
+    A = _matrix(name)
+    lu = _factor(A, dense_lookahead=64)
+    assert lu.stats["dense_tail"] > 64
+    ref, p = _reference(lu)
+    err = col_max_rel(lu.lu_values(), ref, p["sym_c_ptr"])
+    assert err <= FACTOR_TOL, err
+    n = A[3]
+    b = synth.rhs_uniform(n, 1, seed=6)[0]
+    x = lu.solve(b, refine=True, tol=1e-12, maxiter=30)
+    M = sp.csc_matrix(A[:3], shape=(n, n))
+    assert np.linalg.norm(M @ x - b) / np.linalg.norm(b) <= 1e-10
