@@ -130,11 +130,25 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan
     const uint32_t s = md.x, w = md.y, lbase = md.z, m = md.w, t = bi.y;
     const uint32_t l = s + w - 1;
     const uint32_t tid = threadIdx.x, n = P.n;
-    // L11, strictly lower: L(s+k, s+c) at diag[s+c] + (k - c)
-    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
-        const uint32_t c = e / w, k = e - c * w;
-        if (k > c) sT[c * kLD + k] = __ldg(val + P.diag[s + c] + (k - c));
+    __shared__ uint32_t sB[kSnMaxWidth];
+    if (tid < w) sB[tid] = P.diag[s + tid];
+    __syncthreads();
+    // L11, strictly lower: L(s+k, s+c) at diag[s+c] + (k - c); eight loads in flight per thread
+    for (uint32_t e0 = 0; e0 < w * kSnMaxWidth; e0 += 8 * 256) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t e = e0 + u * 256 + tid, c = e >> 6, k = e & 63;
+            v[u] = (c < w && k < w && k > c) ? __ldg(val + sB[c] + (k - c)) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t e = e0 + u * 256 + tid, c = e >> 6, k = e & 63;
+            if (c < w && k < w && k > c) sT[c * kLD + k] = v[u];
+        }
     }
+    __syncthreads();
+    if (tid < w) sB[tid] += l + 1 - (s + tid);  // L21(r, c) at sB[c] + r
     __syncthreads();
     const uint32_t r = t * blockDim.x + tid;  // L21 row of this thread
     for (uint32_t q = 0; q < nrhs; ++q) {
@@ -158,7 +172,14 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan
         __syncthreads();
         if (r < m) {
             float acc = 0.0f;
-            for (uint32_t c = 0; c < w; ++c) acc = fmaf(__ldg(val + P.diag[s + c] + (l + 1 - (s + c)) + r), xs[c], acc);
+            for (uint32_t c0 = 0; c0 < w; c0 += 16) {
+                float v[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) v[u] = (c0 + u < w) ? __ldg(val + sB[c0 + u] + r) : 0.0f;
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                    if (c0 + u < w) acc = fmaf(v[u], xs[c0 + u], acc);
+            }
             if (acc != 0.0f) atomicAdd(yq + __ldg(P.ridx + lbase + r), -acc);
         }
         __syncthreads();
@@ -178,19 +199,50 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
     }
     const uint32_t s = W.meta[bi.x].x, w = W.meta[bi.x].y, t = bi.y;
     const uint32_t tid = threadIdx.x, n = P.n;
-    // U11 with its diagonal: U(s+k, s+c), k <= c, at diag[s+c] - (c - k)
-    for (uint32_t e = tid; e < w * w; e += blockDim.x) {
-        const uint32_t c = e / w, k = e - c * w;
-        if (k <= c) sT[c * kLD + k] = __ldg(val + P.diag[s + c] - (c - k));
-    }
-    if (tid == 0) {
+    __shared__ uint32_t sB[kSnMaxWidth], sC[kSnMaxWidth];
+    if (tid < 32) {
         // entries of column s+c above the block: positions cptr[s+c] .. diag[s+c]-c-1
-        uint32_t acc = 0;
-        for (uint32_t c = 0; c < w; ++c) {
-            pre[c] = acc;
-            acc += (P.diag[s + c] - c) - P.cptr[s + c];
+        const uint32_t c0 = tid, c1 = tid + 32;
+        const uint32_t d0 = c0 < w ? P.diag[s + c0] : 0u, d1 = c1 < w ? P.diag[s + c1] : 0u;
+        const uint32_t p0 = c0 < w ? P.cptr[s + c0] : 0u, p1 = c1 < w ? P.cptr[s + c1] : 0u;
+        if (c0 < w) {
+            sB[c0] = d0;
+            sC[c0] = p0;
         }
-        pre[w] = acc;
+        if (c1 < w) {
+            sB[c1] = d1;
+            sC[c1] = p1;
+        }
+        const uint32_t n0 = c0 < w ? (d0 - c0) - p0 : 0u, n1 = c1 < w ? (d1 - c1) - p1 : 0u;
+        uint32_t a0 = n0, a1 = n1;  // inclusive warp scans
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y0 = __shfl_up_sync(0xffffffffu, a0, o), y1 = __shfl_up_sync(0xffffffffu, a1, o);
+            if (tid >= uint32_t(o)) {
+                a0 += y0;
+                a1 += y1;
+            }
+        }
+        const uint32_t tot0 = __shfl_sync(0xffffffffu, a0, 31);
+        if (c0 < w) pre[c0] = a0 - n0;
+        if (c1 < w) pre[c1] = tot0 + a1 - n1;
+        if (c0 == w - 1) pre[w] = a0;
+        if (c1 == w - 1) pre[w] = tot0 + a1;
+    }
+    __syncthreads();
+    // U11 with its diagonal: U(s+k, s+c), k <= c, at diag[s+c] - (c - k); eight loads in flight
+    for (uint32_t e0 = 0; e0 < w * kSnMaxWidth; e0 += 8 * 256) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t e = e0 + u * 256 + tid, c = e >> 6, k = e & 63;
+            v[u] = (c < w && k <= c) ? __ldg(val + sB[c] - (c - k)) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t e = e0 + u * 256 + tid, c = e >> 6, k = e & 63;
+            if (c < w && k <= c) sT[c * kLD + k] = v[u];
+        }
     }
     __syncthreads();
     const uint32_t e0 = t * kSnSweepAbove, e1 = min(e0 + kSnSweepAbove, pre[w]);
@@ -215,20 +267,35 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
             }
         }
         __syncthreads();
-        for (uint32_t e = e0 + tid; e < e1; e += blockDim.x) {
-            uint32_t lo = 0, hi = w;  // last c with pre[c] <= e
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (pre[mid] <= e)
-                    lo = mid;
-                else
-                    hi = mid;
+        // kSnSweepAbove / 256 entries per thread: all loads first, then the atomics
+        constexpr int kPer = int(kSnSweepAbove / 256);
+        uint32_t tg[kPer];
+        float pv[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const uint32_t e = e0 + tid + u * 256;
+            tg[u] = 0xffffffffu;
+            pv[u] = 0.0f;
+            if (e < e1) {
+                uint32_t lo = 0, hi = w;  // last c with pre[c] <= e
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (pre[mid] <= e)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                const float xc = xs[lo];
+                if (xc != 0.0f) {
+                    const uint32_t p = sC[lo] + (e - pre[lo]);
+                    tg[u] = __ldg(P.ridx + p);
+                    pv[u] = __fmul_rn(__ldg(val + p), xc);
+                }
             }
-            const float xc = xs[lo];
-            if (xc == 0.0f) continue;
-            const uint32_t p = P.cptr[s + lo] + (e - pre[lo]);
-            atomicAdd(yq + __ldg(P.ridx + p), -__fmul_rn(__ldg(val + p), xc));
         }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u)
+            if (tg[u] != 0xffffffffu) atomicAdd(yq + tg[u], -pv[u]);
         __syncthreads();
     }
 }
