@@ -148,11 +148,15 @@ def cpu_reference(W, steps, warmup, sample_only=False):
     nl = oracle.RefNicsLU(data, indices, indptr, n, threads)
     per_step_solves = W["nrhs"] if sample_only or W["batch"] == 1 else W["nrhs"]
 
+    x_check = {}
+
     def step(i):
         nl.refactor(vals[i % 2])
         for k in range(W["nrhs"]):
             x = nl.solve(b[k])
             nl.refine(x, b[k], W["tol"], 10)
+            if i % 2 == 0 and k == 0:
+                x_check["x"] = np.array(x, dtype=np.float64, copy=True)
 
     for i in range(warmup):
         step(i)
@@ -162,7 +166,41 @@ def cpu_reference(W, steps, warmup, sample_only=False):
     dt = (time.perf_counter() - t0) / steps
     sample = (f"{steps} step(s) of NICSLU ReFactorize_MT + Solve + Refine on one value set "
               f"({per_step_solves} RHS) of the workload matrix")
-    return per_step_solves / dt, dt, threads, sample
+    if not x_check:  # the timed steps factored value set 1 only
+        nl.refactor(vals[0])
+        x = nl.solve(b[0])
+        nl.refine(x, b[0], W["tol"], 10)
+        x_check["x"] = np.array(x, dtype=np.float64, copy=True)
+    return per_step_solves / dt, dt, threads, sample, x_check["x"]
+
+
+def plain_form(W, vals, local, nrhs):
+    """The plain unbatched, unrefined FP32 form on the batch's pattern: one
+    value set factored alone, then one FP32 solve of its right-hand sides,
+    device-resident, timed per matrix."""
+    import torch
+
+    import pyglu
+
+    data, indices, indptr, n = W["A"]
+    lu = pyglu.GLUFactorization(vals[0], indices, indptr, n, device=local)
+    dev = torch.device("cuda", local)
+    d = [torch.tensor(vals[i], dtype=torch.float64, device=dev) for i in range(2)]
+    b = torch.tensor(W["b"](n, nrhs, 11), dtype=torch.float32, device=dev)
+    x = torch.empty_like(b)
+    ts = []
+    for i in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lu.refactor_device(d[i % 2])
+        lu.solve_device(b, x, refine=False)
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    return {"value": nrhs / (ms / 1e3), "unit": "solves/s", "ms_per_matrix": ms,
+            "form": "one value set: FP32 refactor + FP32 solve of its right-hand sides, no refinement"}
 
 
 def main():
@@ -172,7 +210,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        v, dt, thr, sample = cpu_reference(W, args.steps, args.warmup)
+        v, dt, thr, sample, _ = cpu_reference(W, args.steps, args.warmup)
         line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
@@ -263,6 +301,16 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     solve_ms = e0.elapsed_time(e1)
+
+    # refined solution of value set 0, RHS 0, for the forward-error check
+    x_check = None
+    if B == 1:
+        _capi.check(eng.glu_load_source_values(handle, 0, 1, _capi.C.c_void_p(d_vals[0].data_ptr()), _capi.GLU_DEVICE, sp_))
+        _capi.check(eng.glu_factor(handle, 0, 1, 0, sp_), "factor")
+        s = eng.glu_solve_refined(handle, 0, 1, nrhs, _capi.C.c_void_p(d_b.data_ptr()), _capi.C.c_void_p(d_x.data_ptr()),
+                                  W["tol"], 10, 0, _capi.GLU_DEVICE, _capi.C.byref(rst), sp_)
+        torch.cuda.synchronize()
+        x_check = d_x[0, 0].double().cpu().numpy().copy()
 
     # e2e through the public API with host buffers
     e2e_steps = max(1, min(args.steps, 5))
@@ -355,6 +403,30 @@ def main():
               "sn_update_flops": float(st.sn_update_flops) * B}
     sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    peak_c = _capi.C.c_double(0.0)
+    fp32_meas = fp32_peak
+    if eng.glu_measure_fp32_peak(local, _capi.C.byref(peak_c)) == 0 and peak_c.value > 0:
+        fp32_meas = peak_c.value
+    # whole-refactorization roofline, both bounds: HBM with 16 B per LU entry
+    # ((8 B + 8) per entry for a batch of B) and FP32 with sum |L_k| + 2|L_k||U_k|
+    fac_bytes = (16.0 * nnz_lu) if B == 1 else (8.0 * B + 8.0) * nnz_lu
+    fac_gbs = fac_bytes / (factor_ms / 1e3) / 1e9
+    fac_tf = flops / (factor_ms / 1e3) / 1e12
+    factor_roof = {"hbm": {"algorithmic_bytes": fac_bytes, "achieved_gbs": fac_gbs, "peak_gbs": hbm,
+                           "frac": fac_gbs / hbm},
+                   "fp32": {"flops": flops, "achieved_tflops": fac_tf, "peak_tflops": fp32_meas,
+                            "peak_source": "measured FFMA microbenchmark (glu_measure_fp32_peak)",
+                            "frac": fac_tf / fp32_meas},
+                   "binding": "fp32" if fac_tf / fp32_meas >= fac_gbs / hbm else "hbm",
+                   "levels": int(st.num_lev), "supernode_levels": int(st.sn_levels),
+                   "levels_per_s": st.num_lev / (factor_ms / 1e3)}
+    # refined solve: each FP32 solve reads the factors once (8 B per LU entry)
+    # plus 16 B per unknown per RHS, each residual 12 B per A entry per RHS
+    nnz_a = len(data)
+    nsolves = iters + 1
+    sol_bytes = B * (nsolves * (8.0 * nnz_lu + 16.0 * n * nrhs) + iters * 12.0 * nnz_a * nrhs)
+    solve_roof = {"algorithmic_bytes": sol_bytes, "achieved_gbs": sol_bytes / (solve_ms / 1e3) / 1e9,
+                  "frac": sol_bytes / (solve_ms / 1e3) / 1e9 / hbm, "fp32_solves": nsolves, "residuals": iters}
     roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": traffic, "traffic_source": traffic_note, "kernel": dom, "launches": dom_n,
             "kernel_ms": dom_ms, **sn_alg,
@@ -377,7 +449,12 @@ def main():
             "refine_iterations": iters, "refine_dtype": "f64",
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": roof, "gpu_launches": int(st.factor_launches) * args.steps, "clocks": clk}
+            "roofline": roof, "factor_roofline": factor_roof, "solve_roofline": solve_roof,
+            "residual_inf": rst.residual_inf,
+            "gpu_launches": int(st.factor_launches) * args.steps, "clocks": clk}
+    if B > 1:
+        line["plain_form"] = plain_form(W, vals, local, nrhs)
+        line["plain_form"]["batched_over_plain"] = value / line["plain_form"]["value"]
     if rank == 0 and world == 1 and B == 1 and args.reference_gpu:
         # the reference's own numeric.cu (LUonDevice) on the same arrays and values
         try:
@@ -407,9 +484,17 @@ def main():
             import oracle
 
             if oracle.ref_available():
-                v, dt, thr, sample = cpu_reference(W, 1, 0, sample_only=True)
+                v, dt, thr, sample, x_ref = cpu_reference(W, 1, 0, sample_only=True)
                 line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": thr, "kind": "reference",
                                         "sample": sample}
+                if B == 1 and x_check is not None:
+                    # forward error of the GPU's refined solution against NICSLU's
+                    # FP64 refined solution of the same system (value set 0, RHS 0)
+                    dx = x_check - x_ref
+                    line["forward_error"] = {
+                        "vs": "NICSLU FP64 factor + refinement on the host",
+                        "rel_2": float(np.linalg.norm(dx) / np.linalg.norm(x_ref)),
+                        "rel_inf": float(np.abs(dx).max() / np.abs(x_ref).max())}
         except Exception as e:  # pragma: no cover
             line["cpu_baseline"] = {"error": str(e)}
     if rank == 0:

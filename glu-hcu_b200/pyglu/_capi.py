@@ -36,7 +36,7 @@ ENGINE_SYMBOLS = [
     "glu_set_source", "glu_load_lu_values", "glu_store_lu_values", "glu_load_source_values",
     "glu_factor", "glu_solve", "glu_solve_transposed", "glu_solve_refined", "glu_get_stats",
     "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
-    "glu_kernel_kind_name",
+    "glu_kernel_kind_name", "glu_measure_fp32_peak",
 ]
 GLU_KERNEL_KINDS = 12
 PRE_SYMBOLS = [
@@ -121,6 +121,7 @@ def load_engine():
         "glu_solve_noalloc": [_vp, _u32, _u32, _vp, _vp, _vp],
         "glu_profile_enable": [_vp, C.c_int],
         "glu_kernel_times": [_vp, _vp, _vp],
+        "glu_measure_fp32_peak": [C.c_int, C.POINTER(C.c_double)],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

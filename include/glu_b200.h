@@ -216,6 +216,11 @@ glu_status glu_profile_enable(glu_handle_t h, int on);
 glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
 const char *glu_kernel_kind_name(int kind);
 
+/* FP32 fused multiply-add throughput of a device in TFLOP/s (a short
+ * microbenchmark, about a second), the compute bound of the factorization's
+ * roofline.  No counterpart in the reference. */
+glu_status glu_measure_fp32_peak(int device, double *tflops);
+
 /* Schedule knobs (the autotuner's search space).  Applies to later calls. */
 typedef struct {
     uint32_t wide_work;        /* a level with more update work runs alone       */
