@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="mesh", choices=["mesh", "nodal", "batch"])
+    p.add_argument("--workload", default="mesh", choices=["mesh", "nodal", "batch", "uneven"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--reference-gpu", action="store_true",
                    help="also time the reference's own numeric.cu (LUonDevice) on the same arrays")
@@ -60,6 +60,12 @@ def workload(name, side=700):
         A = synth.config0()
         return dict(A=A, batch=1, nrhs=1, tol=1e-10, values=2,
                     desc="nodal matrix n=4960, 1 RHS, refine to 1e-10",
+                    b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
+    if name == "uneven":  # the reference arm times one system of the set (its largest)
+        n, k, sd = max(synth.config3_systems(count=64, seed=0, n_range=(2000, 12000), rhs_range=(1, 64)))
+        A = synth.nodal(n, seed=sd)
+        return dict(A=A, batch=1, nrhs=k, tol=1e-10, values=2,
+                    desc=f"largest system of the uneven batch, n={n}, {k} RHS, refine to 1e-10",
                     b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
     A = synth.config2_pattern()
     return dict(A=A, batch=256, nrhs=4, tol=1e-10, values=1,
@@ -174,6 +180,54 @@ def cpu_reference(W, steps, warmup, sample_only=False):
     return per_step_solves / dt, dt, threads, sample, x_check["x"]
 
 
+def run_uneven(args, world, rank, local):
+    """Uneven batch: 64 independent nodal systems of different sizes, each with
+    1-64 right-hand sides, refactored and FP64-refined together (UnevenBatch,
+    one stream per worker thread, host buffers)."""
+    import torch
+
+    import pyglu
+    from pyglu import synth
+
+    torch.cuda.set_device(local)
+    specs = synth.config3_systems(count=64, seed=0, n_range=(2000, 12000), rhs_range=(1, 64))
+    systems = [synth.nodal(n, seed=sd) for n, k, sd in specs]
+    bs = [synth.rhs_uniform(n, k, seed=sd).T.copy() for n, k, sd in specs]
+    vals = [synth.perturb_values(*A, count=2, seed=7) for A in systems]
+    ub = pyglu.UnevenBatch(systems, workers=16, device=local)
+    solves = sum(k for _, k, _ in specs)
+
+    def step(i):
+        ub.refactor([v[i % 2] for v in vals])
+        return ub.solve(bs, tol=1e-10)
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        xs = step(i)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    res = max(st["residual"] for st in ub.last_refine)
+    h2d = sum(v[0].nbytes for v in vals) + sum(b.nbytes for b in bs)
+    d2h = sum(x.nbytes for x in xs)
+    value = world * solves / (ms / 1e3)
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 nodal systems, n log-uniform in [2,000, 12,000] (the uneven-batch "
+                                   "shape at reduced sizes), 1-64 RHS each, refine to 1e-10",
+                       "systems": len(specs), "rhs_total": solves, "n_total": sum(n for n, _, _ in specs),
+                       "parallelism": f"16 streams x{world}"},
+            "residual": res, "refine_dtype": "f64",
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "note": "the uneven batch is driven through host buffers; value is already end to end"},
+            "roofline": None, "gpu_launches": None, "clocks": None}
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def plain_form(W, vals, local, nrhs):
     """The plain unbatched, unrefined FP32 form on the batch's pattern: one
     value set factored alone, then one FP32 solve of its right-hand sides,
@@ -206,6 +260,11 @@ def plain_form(W, vals, local, nrhs):
 def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
+    if args.workload == "uneven" and args.impl == "ours":
+        run_uneven(args, world, rank, local)
+        if pg:
+            pg.destroy_process_group()
+        return
     W = workload(args.workload, args.side)
     if args.impl == "reference":
         if rank != 0:

@@ -35,7 +35,7 @@ except ImportError:  # pragma: no cover
 from . import _capi
 from ._capi import GLUError, NotConvergedError, SingularMatrixError, check, ptr
 
-__all__ = ["splu", "spsolve", "GLUFactorization", "BatchedGLU", "sparse_solve", "tune",
+__all__ = ["splu", "spsolve", "GLUFactorization", "BatchedGLU", "UnevenBatch", "sparse_solve", "tune",
            "GLUError", "SingularMatrixError", "NotConvergedError", "read_mtx"]
 
 
@@ -414,6 +414,94 @@ class BatchedGLU:
         st = _capi.Stats()
         _capi.engine().glu_get_stats(self._eng._h, _capi.C.byref(st))
         return {k: getattr(st, k) for k, _ in _capi.Stats._fields_}
+
+
+class UnevenBatch:
+    """Independent systems of different sizes and patterns, each with its own
+    right-hand sides, refactored and solved together.
+
+    ``systems`` is a list of CSC matrices ``(data, indices, indptr, n)``.  Every
+    system keeps its own analysis, handle and CUDA stream; ``workers`` host
+    threads drive them, so the launches of different systems overlap on the
+    GPU (the engine's calls release the GIL).  The same FP32 factorization and
+    FP64 refinement as ``GLUFactorization`` apply to each system; ``refactor``
+    keeps each system's ordering and scaling, as a refactorization does.
+    """
+
+    def __init__(self, systems, perturb=False, device=0, workers=8):
+        torch = _torch()
+        self.lus = [GLUFactorization(*sys_, perturb=perturb, device=device) for sys_ in systems]
+        self.workers = max(1, min(int(workers), len(self.lus)))
+        self._streams = [torch.cuda.Stream(device=device) for _ in range(self.workers)]
+        self.perturb = bool(perturb)
+        self.last_refine = None
+
+    def __len__(self):
+        return len(self.lus)
+
+    def _run(self, fn):
+        import concurrent.futures as cf
+
+        with cf.ThreadPoolExecutor(self.workers) as ex:
+            futs = [ex.submit(self._worker, w, fn) for w in range(self.workers)]
+            out = {}
+            for f in futs:
+                out.update(f.result())
+        return [out[i] for i in range(len(self.lus))]
+
+    def _worker(self, w, fn):
+        st = _capi.C.c_void_p(self._streams[w].cuda_stream)
+        return {i: fn(i, st) for i in range(w, len(self.lus), self.workers)}
+
+    def refactor(self, values):
+        """New values for every system (a list of data arrays, CSC order)."""
+        eng = _capi.engine()
+        if len(values) != len(self.lus):
+            raise ValueError(f"expected {len(self.lus)} value arrays, got {len(values)}")
+        vals = [np.ascontiguousarray(v, dtype=np.float64) for v in values]
+        for v, lu in zip(vals, self.lus):
+            if v.shape != (lu._an.nnz_a,):
+                raise ValueError(f"expected {lu._an.nnz_a} values, got shape {v.shape}")
+
+        def fn(i, st):
+            lu = self.lus[i]
+            check(eng.glu_load_source_values(lu._eng._h, 0, 1, ptr(vals[i]), _capi.GLU_HOST, st), "value upload")
+            check(eng.glu_factor(lu._eng._h, 0, 1, 1 if self.perturb else 0, st), "GPU factorization")
+            return None
+
+        self._run(fn)
+        return self
+
+    def solve(self, bs, tol=1e-10, maxiter=10):
+        """FP64-refined solves: ``bs[i]`` has shape (n_i,) or (n_i, k_i);
+        returns the list of solutions in the same shapes."""
+        eng = _capi.engine()
+        if len(bs) != len(self.lus):
+            raise ValueError(f"expected {len(self.lus)} right-hand sides, got {len(bs)}")
+        mats = []
+        for b, lu in zip(bs, self.lus):
+            b = np.asarray(b, dtype=np.float64)
+            if b.shape[0] != lu.n:
+                raise ValueError(f"RHS length {b.shape[0]} != matrix dimension {lu.n}")
+            mats.append((b.ndim == 1, np.ascontiguousarray(b.reshape(lu.n, -1).T)))
+        stats = [None] * len(self.lus)
+
+        def fn(i, st):
+            lu = self.lus[i]
+            vec, bm = mats[i]
+            x = np.empty_like(bm)
+            rs = _capi.RefineStats()
+            s = eng.glu_solve_refined(lu._eng._h, 0, 1, bm.shape[0], ptr(bm), ptr(x), float(tol), int(maxiter), 0,
+                                      _capi.GLU_HOST, _capi.C.byref(rs), st)
+            if s != _capi.GLU_ERR_NOT_CONVERGED:
+                check(s, "refined solve")
+            stats[i] = dict(iterations=rs.iterations, residual=rs.residual, residual_inf=rs.residual_inf)
+            x = x.T
+            return np.ascontiguousarray(x[:, 0] if vec else x)
+
+        xs = self._run(fn)
+        self.last_refine = stats
+        return xs
 
 
 def write_mtx(path, data, indices, indptr, n):
