@@ -1334,67 +1334,72 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         GLU_LAUNCH(KK_DGATHER,
                    launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
                    "factor (dense gather)");
-    // Look-ahead (trailing blocks of tune.dense_lookahead columns or more): the panels
-    // and, after the panel at k0, the next panel's row and column strips of the
-    // trailing update run on a high-priority internal stream; the rest of the
-    // update runs on st, concurrently with the next panel, which it does not
-    // touch.  The strips of step p+1 wait for the rest of step p (the same
-    // entries, updated in step order).
+    // Small trailing blocks: panel, update, one panel at a time.  Large ones
+    // (tune.dense_lookahead columns or more) take the panels in pairs: panel
+    // k0, the second panel's row and column strips of its update (K = 64),
+    // panel k0 + 64, then one update of the rest with both panels (K = 128:
+    // every entry still receives its products in column order, C read and
+    // written once per pair).  The panels and the strips run on a
+    // high-priority internal stream, the rest of the pair's update on st,
+    // concurrently with the next pair's first panel, which it does not touch;
+    // the next strips wait for it (the same entries, updated in column order).
     const bool lookahead = h->aux && h->tune.dense_lookahead && h->m >= h->tune.dense_lookahead && h->m > kDenseNB;
     const uint32_t *doff = h->d_doff.as<uint32_t>();
     float *dscr = h->d_diag_scratch.as<float>();
-    if (!lookahead) {
-        for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
-            const uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
-            const uint32_t rest = h->m - (k0 + kb);
-            GLU_LAUNCH(KK_PANEL, launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, st),
-                       "factor (dense panel)");
-            GLU_LAUNCH(KK_UPDATE,
-                       launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
-                                           DenseRegion{0, rest, 0, rest, 1}, st),
-                       "factor (dense update)");
-        }
-    } else {
-        cudaStream_t hp = h->aux;
+    cudaStream_t ps = lookahead ? h->aux : st;  // panels and strips
+    bool rest_pending = false;
+    if (lookahead) {
         GLU_CUDA(cudaEventRecord(h->ev_fork, st), "event");
-        GLU_CUDA(cudaStreamWaitEvent(hp, h->ev_fork, 0), "stream wait");
-        bool rest_pending = false;
-        const uint32_t nb = kDenseNB;
-        for (uint32_t k0 = 0; k0 < h->m; k0 += kDenseNB) {
-            const uint32_t kb = std::min<uint32_t>(kDenseNB, h->m - k0);
-            const uint32_t rest = h->m - (k0 + kb);
-            GLU_CUDA(pf.begin(hp), "profile event");
-            GLU_CUDA(launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, hp),
-                     "factor (dense panel)");
-            GLU_CUDA(pf.end(KK_PANEL, hp), "profile event");
-            if (rest_pending) GLU_CUDA(cudaStreamWaitEvent(hp, h->ev_rest, 0), "stream wait");
-            if (rest <= nb) {  // last steps: the whole update after the panel
-                GLU_CUDA(pf.begin(hp), "profile event");
-                GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
-                                             DenseRegion{0, rest, 0, rest, 1}, hp),
-                         "factor (dense update)");
-                GLU_CUDA(pf.end(KK_UPDATE, hp), "profile event");
-                rest_pending = false;
-                continue;
-            }
-            GLU_CUDA(cudaEventRecord(h->ev_panel, hp), "event");
-            GLU_CUDA(pf.begin(hp), "profile event");
-            GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, DenseRegion{0, nb, 0, rest, 1},
-                                         hp),
-                     "factor (dense update)");
-            GLU_CUDA(launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
-                                         DenseRegion{nb, rest, 0, nb, 0}, hp),
-                     "factor (dense update)");
-            GLU_CUDA(pf.end(KK_UPDATE, hp), "profile event");
+        GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_fork, 0), "stream wait");
+    }
+    const uint32_t nb = kDenseNB;
+    auto update = [&](uint32_t k0, uint32_t kb, DenseRegion reg, cudaStream_t s) -> cudaError_t {
+        cudaError_t e = pf.begin(s);
+        if (e == cudaSuccess) e = launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, reg, s);
+        if (e == cudaSuccess) e = pf.end(KK_UPDATE, s);
+        return e;
+    };
+    auto panel = [&](uint32_t k0, uint32_t kb) -> cudaError_t {
+        cudaError_t e = pf.begin(ps);
+        if (e == cudaSuccess) e = launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, ps);
+        if (e == cudaSuccess) e = pf.end(KK_PANEL, ps);
+        return e;
+    };
+    for (uint32_t k0 = 0; k0 < h->m;) {
+        const uint32_t kb0 = std::min<uint32_t>(nb, h->m - k0);
+        const uint32_t rest0 = h->m - (k0 + kb0);
+        GLU_CUDA(panel(k0, kb0), "factor (dense panel)");
+        if (rest_pending) {
+            GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
+            rest_pending = false;
+        }
+        if (rest0 <= nb || !lookahead) {  // small trailing blocks, last panels: plain steps
+            GLU_CUDA(update(k0, kb0, DenseRegion{0, rest0, 0, rest0, 1, k0}, ps), "factor (dense update)");
+            k0 += kb0;
+            continue;
+        }
+        // the second panel's strips, then the second panel
+        const uint32_t k1 = k0 + nb, kb1 = std::min<uint32_t>(nb, h->m - k1);
+        GLU_CUDA(update(k0, kb0, DenseRegion{0, nb, 0, rest0, 1, k0}, ps), "factor (dense update)");
+        GLU_CUDA(update(k0, kb0, DenseRegion{nb, rest0, 0, nb, 0, k0}, ps), "factor (dense update)");
+        GLU_CUDA(panel(k1, kb1), "factor (dense panel)");
+        const uint32_t rest1 = h->m - (k1 + kb1), kk = kb0 + kb1;
+        if (rest1 <= nb) {
+            GLU_CUDA(update(k0, kk, DenseRegion{0, rest1, 0, rest1, 1, k1}, ps), "factor (dense update)");
+        } else {
+            GLU_CUDA(cudaEventRecord(h->ev_panel, ps), "event");
+            GLU_CUDA(update(k0, kk, DenseRegion{0, nb, 0, rest1, 1, k1}, ps), "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, 0, nb, 0, k1}, ps), "factor (dense update)");
             GLU_CUDA(cudaStreamWaitEvent(st, h->ev_panel, 0), "stream wait");
-            GLU_LAUNCH(KK_UPDATE,
-                       launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr,
-                                           DenseRegion{nb, rest, nb, rest, 0}, st),
-                       "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, nb, rest1, 0, k1}, st), "factor (dense update)");
             GLU_CUDA(cudaEventRecord(h->ev_rest, st), "event");
             rest_pending = true;
         }
-        GLU_CUDA(cudaEventRecord(h->ev_fork, hp), "event");
+        k0 = k1 + kb1;
+    }
+    if (lookahead) {
+        if (rest_pending) GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
+        GLU_CUDA(cudaEventRecord(h->ev_fork, ps), "event");
         GLU_CUDA(cudaStreamWaitEvent(st, h->ev_fork, 0), "stream wait");
     }
     if (h->m && h->dense_buffer)

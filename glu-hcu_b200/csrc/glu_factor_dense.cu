@@ -260,10 +260,13 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     float *val = val_base + blockIdx.z * stride;
     const uint32_t tid = threadIdx.x;
     if (reg.writeback && blockIdx.x == 0 && blockIdx.y == 0) {
+        // the factored diagonal block of the panel at wb_k0, kept in scratch
+        // while that panel's blocks still read the original
         const float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
-        for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
-            uint32_t c = e / kb, r = e - c * kb;
-            st_cg(val + doff[k0 + c] + k0 + r, ds[c * kDenseNB + r]);
+        const uint32_t wk = reg.wb_k0, wb = min(uint32_t(kDenseNB), m - wk);
+        for (uint32_t e = tid; e < wb * wb; e += blockDim.x) {
+            uint32_t c = e / wb, r = e - c * wb;
+            st_cg(val + doff[wk + c] + wk + r, ds[c * kDenseNB + r]);
         }
     }
     const uint32_t r0 = k0 + kb;
@@ -291,44 +294,49 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
 #pragma unroll
         for (int i = 0; i < RM; ++i) acc[i][j] = sC[(tx * RM + j) * LDC + ty * RM + i];
     __syncthreads();
-    // stage L21 tile: sA[k][row]
+    // K = kb (one or two panels) in chunks of kDenseNB, in increasing k
+    for (uint32_t kc = 0; kc < kb; kc += kDenseNB) {
+        const uint32_t kn = min(uint32_t(kDenseNB), kb - kc);
+        // stage L21 tile: sA[k][row]
 #pragma unroll 16
-    for (uint32_t e = tid; e < uint32_t(kDenseNB) * TB; e += 256) {
-        uint32_t k = e / TB, row = e - k * TB;
-        float v = 0.0f;
-        if (k < kb && rbase + row < rlim) v = ld_cg(val + doff[k0 + k] + r0 + rbase + row);
-        sA[k * TB + row] = v;
-    }
-    // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
-    {
-        uint32_t lane = tid & 31, w = tid >> 5;
+        for (uint32_t e = tid; e < uint32_t(kDenseNB) * TB; e += 256) {
+            uint32_t k = e / TB, row = e - k * TB;
+            float v = 0.0f;
+            if (k < kn && rbase + row < rlim) v = ld_cg(val + doff[k0 + kc + k] + r0 + rbase + row);
+            sA[k * TB + row] = v;
+        }
+        // stage U12 tile: sB[k][col]; lanes run along k (contiguous in memory)
+        {
+            uint32_t lane = tid & 31, w = tid >> 5;
 #pragma unroll 8
-        for (uint32_t col = w; col < uint32_t(TB); col += 8) {
-            bool cok = cbase + col < mp;
-            const float *src = cok ? val + doff[r0 + cbase + col] + k0 : nullptr;
+            for (uint32_t col = w; col < uint32_t(TB); col += 8) {
+                bool cok = cbase + col < mp;
+                const float *src = cok ? val + doff[r0 + cbase + col] + k0 + kc : nullptr;
 #pragma unroll
-            for (uint32_t h = 0; h < uint32_t(kDenseNB); h += 32) {
-                uint32_t k = h + lane;
-                float v = (cok && k < kb) ? ld_cg(src + k) : 0.0f;
-                sB[k * LDB + col] = v;
+                for (uint32_t h = 0; h < uint32_t(kDenseNB); h += 32) {
+                    uint32_t k = h + lane;
+                    float v = (cok && k < kn) ? ld_cg(src + k) : 0.0f;
+                    sB[k * LDB + col] = v;
+                }
             }
         }
-    }
-    __syncthreads();
+        __syncthreads();
 #pragma unroll 4
-    for (uint32_t k = 0; k < kb; ++k) {
-        float av[RM], bv[RM];
+        for (uint32_t k = 0; k < kn; ++k) {
+            float av[RM], bv[RM];
 #pragma unroll
-        for (int q = 0; q < RM; q += 4) {
-            float4 a4 = *reinterpret_cast<const float4 *>(sA + k * TB + ty * RM + q);
-            float4 b4 = *reinterpret_cast<const float4 *>(sB + k * LDB + tx * RM + q);
-            av[q] = a4.x; av[q + 1] = a4.y; av[q + 2] = a4.z; av[q + 3] = a4.w;
-            bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
+            for (int q = 0; q < RM; q += 4) {
+                float4 a4 = *reinterpret_cast<const float4 *>(sA + k * TB + ty * RM + q);
+                float4 b4 = *reinterpret_cast<const float4 *>(sB + k * LDB + tx * RM + q);
+                av[q] = a4.x; av[q + 1] = a4.y; av[q + 2] = a4.z; av[q + 3] = a4.w;
+                bv[q] = b4.x; bv[q + 1] = b4.y; bv[q + 2] = b4.z; bv[q + 3] = b4.w;
+            }
+#pragma unroll
+            for (int i = 0; i < RM; ++i)
+#pragma unroll
+                for (int j = 0; j < RM; ++j) acc[i][j] = fmaf(-av[i], bv[j], acc[i][j]);
         }
-#pragma unroll
-        for (int i = 0; i < RM; ++i)
-#pragma unroll
-            for (int j = 0; j < RM; ++j) acc[i][j] = fmaf(-av[i], bv[j], acc[i][j]);
+        __syncthreads();
     }
     __syncthreads();
 #pragma unroll

@@ -84,11 +84,12 @@ constexpr int kGemmTile = 128;      // trailing-update tile
 cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
                                float *diag_scratch, uint32_t last_has_l, cudaStream_t st);
-// Part of the trailing update after the panel at k0: rows [r_lo, r_hi) and
-// columns [c_lo, c_hi) of the trailing block (relative to k0 + kb); writeback
-// != 0 also stores the factored diagonal block from diag_scratch.
+// Part of the trailing update after the panels [k0, k0 + kb) (kb <= 2 x
+// kDenseNB): rows [r_lo, r_hi) and columns [c_lo, c_hi) of the trailing block
+// (relative to k0 + kb); writeback != 0 also stores the factored diagonal
+// block of the panel at wb_k0 from diag_scratch.
 struct DenseRegion {
-    uint32_t r_lo, r_hi, c_lo, c_hi, writeback;
+    uint32_t r_lo, r_hi, c_lo, c_hi, writeback, wb_k0;
 };
 cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
