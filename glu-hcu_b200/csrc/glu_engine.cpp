@@ -134,7 +134,9 @@ struct SnLevel {
     uint32_t i0, i1;        // supernodes (level order)
     uint32_t pb0, pblocks;  // blocks in the panel map
     uint32_t ub0, ublocks;  // tiles in the update map
-    uint32_t atomic, wide;  // wide: has a supernode of width >= 2
+    uint32_t db0, dblocks;  // blocks in the diagonal-block map (supernodes of width >= 2)
+    uint32_t atomic;
+    uint32_t panel_w;       // widest supernode with a block of its own in the panel map
 };
 struct Step {
     int kind;
@@ -175,7 +177,7 @@ struct glu_handle_s {
     // supernodal plan of the sparse part (used when tune.sn_width != 0)
     bool use_sn = false;
     uint32_t nsn = 0;
-    DevBuf d_sn_meta, d_sn_pmap, d_sn_umap, d_sn_psmall, d_sn_usmall, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
+    DevBuf d_sn_meta, d_sn_dmap, d_sn_dsmall, d_sn_pmap, d_sn_umap, d_sn_psmall, d_sn_usmall, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
     DevBuf d_ss_map[2], d_ss_meta[2], d_ss_small[2];  // supernodal L and U sweeps
@@ -466,14 +468,15 @@ Status build_sn_plan(glu_handle_s *h) {
     }
     std::vector<uint4> meta(ns);
     std::vector<uint2> pmap, umap;
-    std::vector<uint32_t> psmall, usmall, tgt(size_t(ns) + 1, 0);
+    std::vector<uint32_t> psmall, usmall, dsmall, tgt(size_t(ns) + 1, 0);
+    std::vector<uint2> dmap;
     std::vector<uint64_t> pos_off(size_t(ns) + 1, 0);
     const uint32_t PT = kSnPanelThreads, UT = 64, TW = kSnPanelThreads / 32;
     double upd_flops = 0, upd_bytes = 0, pan_bytes = 0;
     for (int32_t l = 0; l < nlev; ++l) {
-        uint32_t updating = 0, wide = 0;
-        const uint32_t pb0 = uint32_t(pmap.size()), ub0 = uint32_t(umap.size());
-        const size_t ps0 = psmall.size(), us0 = usmall.size();
+        uint32_t updating = 0, panel_w = 0;
+        const uint32_t pb0 = uint32_t(pmap.size()), ub0 = uint32_t(umap.size()), db0 = uint32_t(dmap.size());
+        const size_t ps0 = psmall.size(), us0 = usmall.size(), ds0 = dsmall.size();
         for (uint32_t i = lcount[l]; i < lcount[l + 1]; ++i) {
             const uint32_t q = order[i];
             const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
@@ -482,7 +485,11 @@ Status build_sn_plan(glu_handle_s *h) {
             const uint64_t tiles = ((m + UT - 1) / UT) * ((nt + UT - 1) / UT);
             const uint64_t pb = (m + PT - 1) / PT + (w >= 2 ? (nt + TW - 1) / TW : 0);
             if (tiles) ++updating;
-            if (w >= 2) ++wide;
+            // diagonal blocks: a warp each up to kSnSmallWidth (eight to a block), else a block
+            if (w > kSnSmallWidth)
+                dmap.push_back(make_uint2(i, 0u));
+            else if (w >= 2)
+                dsmall.push_back(i);
             if (pmap.size() + pb > UINT32_MAX || umap.size() + tiles > UINT32_MAX ||
                 uint64_t(tgt[i]) + nt > UINT32_MAX)
                 return set_error(GLU_ERR_UNSUPPORTED, "supernodal schedule too large");
@@ -490,8 +497,10 @@ Status build_sn_plan(glu_handle_s *h) {
             const bool small = h->tune.sn_small && w <= kSnSmallWidth && m <= 32 && nt <= 32;
             if (pb && small)
                 psmall.push_back(i);
-            else
+            else if (pb) {
                 for (uint64_t bb = 0; bb < pb; ++bb) pmap.push_back(make_uint2(i, uint32_t(bb)));
+                panel_w = std::max(panel_w, w);
+            }
             if (tiles && small && m * nt <= 256)
                 usmall.push_back(i);
             else
@@ -507,12 +516,17 @@ Status build_sn_plan(glu_handle_s *h) {
                                                                                              psmall.size() - g))));
         for (size_t g = us0; g < usmall.size(); g += 8)
             umap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(8, usmall.size() - g))));
+        for (size_t g = ds0; g < dsmall.size(); g += kSnDiagSmallPerBlock)
+            dmap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(kSnDiagSmallPerBlock,
+                                                                                             dsmall.size() - g))));
         const uint32_t i0 = lcount[l], i1 = lcount[l + 1];
         h->sn_levels.push_back(SnLevel{i0, i1, pb0, uint32_t(pmap.size()) - pb0, ub0, uint32_t(umap.size()) - ub0,
-                                       updating > 1 ? 1u : 0u, wide ? 1u : 0u});
+                                       db0, uint32_t(dmap.size()) - db0, updating > 1 ? 1u : 0u, panel_w});
     }
     h->nsn = ns;
     GLU_CUDA(upload(h->d_sn_meta, meta), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_dmap, dmap), "upload supernodes");
+    GLU_CUDA(upload(h->d_sn_dsmall, dsmall), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pmap, pmap), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_umap, umap), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_psmall, psmall), "upload supernodes");
@@ -520,7 +534,8 @@ Status build_sn_plan(glu_handle_s *h) {
     GLU_CUDA(upload(h->d_sn_tgt_off, tgt), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pos_off, pos_off), "upload supernodes");
     GLU_CUDA(h->d_sn_tgt.alloc(sizeof(uint4) * std::max<uint32_t>(tgt[ns], 1)), "allocate supernode targets");
-    h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),      h->d_sn_pmap.as<uint2>(),  h->d_sn_umap.as<uint2>(),
+    h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),      h->d_sn_dmap.as<uint2>(),  h->d_sn_dsmall.as<uint32_t>(),
+                      h->d_sn_pmap.as<uint2>(),      h->d_sn_umap.as<uint2>(),
                       h->d_sn_psmall.as<uint32_t>(), h->d_sn_usmall.as<uint32_t>(), h->d_sn_tgt_off.as<uint32_t>(),
                       h->d_sn_tgt.as<uint4>(),       nullptr,                    h->d_sn_pos_off.as<uint64_t>()};
     GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
@@ -782,7 +797,7 @@ Status build_plan(glu_handle_s *h) {
     h->stats.sn_levels = uint32_t(h->sn_levels.size());
     uint64_t launches = 2;
     if (h->use_sn) {
-        for (const SnLevel &lv : h->sn_levels) launches += lv.wide + (lv.pblocks ? 1 : 0) + (lv.ublocks ? 1 : 0);
+        for (const SnLevel &lv : h->sn_levels) launches += (lv.dblocks ? 1 : 0) + (lv.pblocks ? 1 : 0) + (lv.ublocks ? 1 : 0);
     } else {
         launches += h->steps.size() + (NL ? 1 : 0);
     }
@@ -1298,12 +1313,12 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     const uint32_t NL = h->use_sn ? 0u : uint32_t(h->levels_h.size());
     if (h->use_sn) {
         for (const SnLevel &lv : h->sn_levels) {
-            if (lv.wide)
-                GLU_LAUNCH(KK_SN_DIAG, launch_sn_diag(h->P, h->SN, val, stride, count, pert, lv.i0, lv.i1, st),
+            if (lv.dblocks)
+                GLU_LAUNCH(KK_SN_DIAG, launch_sn_diag(h->P, h->SN, val, stride, count, pert, lv.db0, lv.dblocks, st),
                            "factor (supernode diagonal blocks)");
             if (lv.pblocks)
                 GLU_LAUNCH(KK_SN_PANEL,
-                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, lv.pb0, lv.pblocks, st),
+                           launch_sn_panel(h->P, h->SN, val, stride, count, pert, lv.pb0, lv.pblocks, lv.panel_w, st),
                            "factor (supernode panels)");
             if (lv.ublocks)
                 GLU_LAUNCH(KK_SN_UPDATE,

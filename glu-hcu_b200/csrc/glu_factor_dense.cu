@@ -9,221 +9,115 @@
 // (src/numeric.cu:10-345) applied to this block is the unpivoted dense LU; it
 // is computed here blocked (panel width kDenseNB):
 //   1. panel:  A11 = L11 U11 (every block factors the small diagonal block in
-//              shared memory), L21 = A21 U11^-1, U12 = L11^-1 A12;
+//              registers), L21 = A21 U11^-1, U12 = L11^-1 A12;
 //   2. update: A22 -= L21 U12 (register-tiled FP32).
 // Each entry receives the same operations as in the column algorithm (FP32,
 // different summation order).  GESP perturbation (numeric.cu:139-140) is
 // applied to every pivot whose column has an L part.
 #include "glu_common.cuh"
 #include "glu_kernels.h"
+#include "glu_tri.cuh"
 
 namespace glu {
 
-// Factor the kb x kb diagonal block at (k0, k0) of the dense block in shared
-// memory sF (column-major, leading dimension kDenseNB+1).  Step c: the pivot
-// is fixed (GESP), every row i > c computes L(i,c) = A(i,c) / d once, then the
-// block's threads update A(i,j), j > c, with a row split into halves between
-// two threads.  Returns with sF holding L11 (unit, strictly lower) and U11.
-__device__ __forceinline__ void factor_diag_block(const float *__restrict__ val,
-                                                  const uint32_t *__restrict__ doff, uint32_t k0,
-                                                  uint32_t kb, uint32_t m, float pert,
-                                                  uint32_t last_has_l, float *sF, float *lcol) {
-    constexpr int LD = kDenseNB + 1;
-    const uint32_t tid = threadIdx.x;
-    // load: consecutive threads take consecutive rows of a column
-    for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
-        uint32_t j = e / kb, i = e - j * kb;
-        sF[j * LD + i] = ld_cg(val + doff[k0 + j] + k0 + i);
-    }
-    __syncthreads();
-    const uint32_t row = tid >> 1, half = tid & 1;  // 64 rows x 2 halves
-    for (uint32_t c = 0; c < kb; ++c) {
-        // a pivot is perturbed only when its column has an L part
-        const bool has_l = (k0 + c + 1 < m) || last_has_l;
-        const float d = sF[c * LD + c];
-        const float de = (has_l && pert > 0.0f && fabsf(d) < pert) ? pert : d;
-        if (half == 0 && row > c && row < kb) {
-            float l = sF[c * LD + row] / de;
-            sF[c * LD + row] = l;
-            lcol[row] = l;
-        }
-        // (a concurrent reader sees d or pert; both give the same de)
-        if (tid == 0 && de != d) sF[c * LD + c] = de;
-        __syncthreads();
-        if (row > c && row < kb) {
-            const float l = lcol[row];
-            for (uint32_t j = c + 1 + half; j < kb; j += 2) sF[j * LD + row] -= l * sF[j * LD + c];
-        }
-        __syncthreads();
-    }
-}
+// Panel step (kb <= kDenseNB columns at k0).  Every block factors the
+// diagonal block itself (tri_diag_lu, 256 threads); block 0 stores it to
+// diag_scratch (the update kernel writes it back, so no block here overwrites
+// an entry another block may still read); blocks [1, 1 + nL) then solve 128
+// rows of L21 (x U11 = a), the rest 128 columns of U12 (L11 x = a), one per
+// thread, chunked (tri_rows_solve).  The rows or columns are copied to shared
+// memory asynchronously while the diagonal block is factored.  blockIdx.z
+// selects the value set.
+constexpr int kPW = kPanelRows + 1;  // leading dimension of the panel work tile
+constexpr size_t kPanelSmem =
+    sizeof(float) * (size_t(kDenseNB) * kPW + size_t(kDenseNB) * kTriML + 2 * kTriMax) + sizeof(uint32_t) * kDenseNB;
+static_assert(kDenseNB == kTriMax, "panel width is the triangular block width");
+static_assert(2 * kPanelRows == kTriThreads, "128 rows per panel block");
 
-// Panel step.  Block 0 stores the factored diagonal block to diag_scratch (the
-// update kernel writes it back, so no block here overwrites an entry another
-// block may still read); blocks [1, 1+nL) compute rows of L21, the rest
-// columns of U12.  blockIdx.z selects the value set.
-// Full-width panel step (kb == kDenseNB), register resident: the diagonal
-// block is factored with every thread holding half a row (32 values) and the
-// pivot rows broadcast through shared memory, one barrier per column; the
-// L21 rows and U12 columns are then solved one per thread with the whole row
-// or column in registers.  Loops over columns are unrolled so that every
-// register index is static.
-__device__ __forceinline__ void factor_diag_regs(const float *__restrict__ val, const uint32_t *__restrict__ doff,
-                                                 uint32_t k0, uint32_t m, float pert, uint32_t last_has_l,
-                                                 float *sF, float (*urow)[kDenseNB]) {
-    constexpr int NB = kDenseNB;
-    constexpr int LD = kDenseNB + 1;
-    const uint32_t tid = threadIdx.x, lane = tid & 31;
-    const uint32_t row = tid >> 1, half = tid & 1;
-    float a[32];
-#pragma unroll
-    for (int jj = 0; jj < 32; ++jj) a[jj] = ld_cg(val + doff[k0 + half * 32 + jj] + k0 + row);
-#pragma unroll
-    for (int c = 0; c < NB; ++c) {
-        const int hc = c >> 5, jc = c & 31;
-        float *u = urow[c & 1];
-        if (row == uint32_t(c)) {
-            if (half == uint32_t(hc)) {
-                // a pivot is perturbed only when its column has an L part
-                const bool has_l = (k0 + c + 1 < m) || last_has_l;
-                float d = a[jc];
-                if (has_l && pert > 0.0f && fabsf(d) < pert) d = pert;
-                a[jc] = d;
-            }
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj)
-                if (int(half) * 32 + jj >= c) u[half * 32 + jj] = a[jj];
-        }
-        __syncthreads();
-        const float lsrc = __shfl_sync(0xffffffffu, a[jc], (lane & ~1u) | uint32_t(hc));
-        if (row > uint32_t(c)) {
-            const float l = lsrc / u[c];
-            if (half == uint32_t(hc)) a[jc] = l;
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj)
-                if (int(half) * 32 + jj > c) a[jj] = fmaf(-l, u[half * 32 + jj], a[jj]);
-        }
-    }
-#pragma unroll
-    for (int jj = 0; jj < 32; ++jj) sF[(half * 32 + jj) * LD + row] = a[jj];
-    __syncthreads();
-}
-
-__global__ void __launch_bounds__(kPanelRows, 3) k_dense_panel_full(float *val_base, uint64_t stride,
-                                                                    const uint32_t *__restrict__ doff, uint32_t m,
-                                                                    uint32_t k0, const float *pert_z,
-                                                                    float *diag_scratch, uint32_t last_has_l,
-                                                                    uint32_t nL) {
-    constexpr int NB = kDenseNB;
-    constexpr int LD = kDenseNB + 1;
-    __shared__ float sF[NB * LD];
-    __shared__ float urow[2][NB];
+__global__ void __launch_bounds__(kTriThreads) k_dense_panel(float *val_base, uint64_t stride,
+                                                             const uint32_t *__restrict__ doff, uint32_t m,
+                                                             uint32_t k0, uint32_t kb, const float *pert_z,
+                                                             float *diag_scratch, uint32_t last_has_l, uint32_t nL) {
+    extern __shared__ float4 psm4[];
+    float *sW = reinterpret_cast<float *>(psm4);  // [k][thread]: rows of L21 or columns of U12
+    float *sM = sW + kDenseNB * kPW;               // U11 (row-major, pivot reciprocals in the padding) or L11^T
+    float(*urow)[kTriMax] = reinterpret_cast<float(*)[kTriMax]>(sM + kDenseNB * kTriML);
+    uint32_t *sCol = reinterpret_cast<uint32_t *>(sM + kDenseNB * kTriML + 2 * kTriMax);
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
-    factor_diag_regs(val, doff, k0, m, pert, last_has_l, sF, urow);
-    const uint32_t r0 = k0 + NB;
-    const uint32_t tid = threadIdx.x;
-    if (blockIdx.x == 0) {
-        float *ds = diag_scratch + size_t(blockIdx.z) * NB * NB;
-        for (uint32_t e = tid; e < NB * NB; e += blockDim.x) {
-            uint32_t c = e / NB, r = e - c * NB;
-            ds[c * NB + r] = sF[c * LD + r];
-        }
-        return;
-    }
-    float a[NB];
-    if (blockIdx.x <= nL) {
-        // row of L21: x U11 = a
-        const uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
-        if (r >= m) return;
-#pragma unroll
-        for (int c = 0; c < NB; ++c) a[c] = ld_cg(val + doff[k0 + c] + r);
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            const float l = a[c] / sF[c * LD + c];
-            a[c] = l;
-#pragma unroll
-            for (int j = c + 1; j < NB; ++j) a[j] = fmaf(-l, sF[j * LD + c], a[j]);
-        }
-#pragma unroll
-        for (int c = 0; c < NB; ++c) st_cg(val + doff[k0 + c] + r, a[c]);
-    } else {
-        // column of U12: L11 x = a
-        const uint32_t j = r0 + (blockIdx.x - 1 - nL) * kPanelRows + tid;
-        if (j >= m) return;
-        float *col = val + doff[j] + k0;
-#pragma unroll
-        for (int r = 0; r < NB; ++r) a[r] = ld_cg(col + r);
-#pragma unroll
-        for (int r = 0; r < NB; ++r) {
-            const float u = a[r];
-#pragma unroll
-            for (int i = r + 1; i < NB; ++i) a[i] = fmaf(-sF[r * LD + i], u, a[i]);
-        }
-#pragma unroll
-        for (int r = 0; r < NB; ++r) st_cg(col + r, a[r]);
-    }
-}
-
-constexpr int kPW = kPanelRows + 1;  // leading dimension of the panel work tile
-constexpr size_t kPanelSmem = sizeof(float) * (size_t(kDenseNB) * (kDenseNB + 1) + kDenseNB + size_t(kDenseNB) * kPW);
-
-__global__ void __launch_bounds__(kPanelRows) k_dense_panel(float *val_base, uint64_t stride,
-                                                            const uint32_t *__restrict__ doff,
-                                                            uint32_t m, uint32_t k0, uint32_t kb,
-                                                            const float *pert_z, float *diag_scratch,
-                                                            uint32_t last_has_l, uint32_t nL) {
-    constexpr int NB = kDenseNB;
-    constexpr int LD = kDenseNB + 1;
-    extern __shared__ float4 psm4[];
-    float *sF = reinterpret_cast<float *>(psm4);  // diagonal block, column-major
-    float *lcol = sF + NB * LD;                   // multipliers of the current step
-    float *sW = lcol + NB;                        // [k][thread]: rows of L21 or columns of U12
-    float *val = val_base + blockIdx.z * stride;
-    float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
-    factor_diag_block(val, doff, k0, kb, m, pert, last_has_l, sF, lcol);
+    const uint32_t tid = threadIdx.x, b = blockIdx.x;
     const uint32_t r0 = k0 + kb;
-    const uint32_t tid = threadIdx.x;
-    if (blockIdx.x == 0) {
-        float *ds = diag_scratch + size_t(blockIdx.z) * NB * NB;
-        for (uint32_t e = tid; e < kb * kb; e += blockDim.x) {
-            uint32_t c = e / kb, r = e - c * kb;
-            ds[c * NB + r] = sF[c * LD + r];
+    if (tid < kb) sCol[tid] = doff[k0 + tid] + k0;
+    // this block's rows (columns) of the panel, in flight during the LU
+    if (b >= 1 && b <= nL) {
+        const uint32_t rb = r0 + (b - 1) * kPanelRows;
+        for (uint32_t e = tid; e < kb * kPanelRows; e += kTriThreads) {
+            const uint32_t c = e / kPanelRows, t = e - c * kPanelRows;
+            if (rb + t < m) tri_async_copy(sW + c * kPW + t, val + doff[k0 + c] + rb + t);
         }
+    } else if (b > nL) {
+        const uint32_t j0 = r0 + (b - 1 - nL) * kPanelRows;
+        const uint32_t ncol = min(uint32_t(kPanelRows), m - j0);
+        for (uint32_t e = tid; e < ncol * kb; e += kTriThreads) {
+            const uint32_t cc = e / kb, rr = e - cc * kb;
+            tri_async_copy(sW + rr * kPW + cc, val + doff[j0 + cc] + k0 + rr);
+        }
+    }
+    tri_async_commit();
+    __syncthreads();
+    // the diagonal block
+    const uint32_t row = tid >> 2, q = tid & 3;
+    float a[kTriChunk];
+#pragma unroll
+    for (int jj = 0; jj < kTriChunk; ++jj) {
+        const uint32_t cc = q * kTriChunk + jj;
+        a[jj] = (row < kb && cc < kb) ? ld_cg(val + sCol[cc] + row) : 0.0f;
+    }
+    // a pivot is perturbed only when its column has an L part
+    tri_diag_lu(a, kb, (r0 < m) || last_has_l, pert, urow);
+    if (b == 0) {
+        float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
+#pragma unroll
+        for (int jj = 0; jj < kTriChunk; ++jj) {
+            const uint32_t cc = q * kTriChunk + jj;
+            if (row < kb && cc < kb) ds[cc * kDenseNB + row] = a[jj];
+        }
+        tri_async_wait();
         return;
     }
-    if (blockIdx.x <= nL) {
-        // row of L21, one per thread: x U11 = a, in the thread's slot of sW
-        const uint32_t r = r0 + (blockIdx.x - 1) * kPanelRows + tid;
-        if (r >= m) return;
-        float *w = sW + tid;
-        for (uint32_t c = 0; c < kb; ++c) w[c * kPW] = ld_cg(val + doff[k0 + c] + r);
-        for (uint32_t c = 0; c < kb; ++c) {
-            const float l = w[c * kPW] / sF[c * LD + c];
-            w[c * kPW] = l;
-            for (uint32_t j = c + 1; j < kb; ++j) w[j * kPW] -= l * sF[j * LD + c];
+    const bool lrows = b <= nL;
+#pragma unroll
+    for (int jj = 0; jj < kTriChunk; ++jj) {
+        const uint32_t cc = q * kTriChunk + jj;
+        if (lrows)
+            sM[row * kTriML + cc] = a[jj];  // M = U11 (row-major)
+        else
+            sM[cc * kTriML + row] = a[jj];  // M = L11^T
+    }
+    if (lrows) {
+        __syncthreads();
+        if (tid < kb) sM[tid * kTriML + kTriMax] = 1.0f / sM[tid * kTriML + tid];
+    }
+    tri_async_wait();
+    __syncthreads();
+    if (tid < kPanelRows) {
+        if (lrows)
+            tri_rows_solve<true>(sW, kPW, tid, sM, kb);
+        else
+            tri_rows_solve<false>(sW, kPW, tid, sM, kb);
+    }
+    __syncthreads();
+    if (lrows) {
+        const uint32_t rb = r0 + (b - 1) * kPanelRows;
+        for (uint32_t e = tid; e < kb * kPanelRows; e += kTriThreads) {
+            const uint32_t c = e / kPanelRows, t = e - c * kPanelRows;
+            if (rb + t < m) st_cg(val + doff[k0 + c] + rb + t, sW[c * kPW + t]);
         }
-        for (uint32_t c = 0; c < kb; ++c) st_cg(val + doff[k0 + c] + r, w[c * kPW]);
     } else {
-        // column of U12, one per thread: L11 x = a (loaded and stored with
-        // consecutive threads on consecutive rows of one column)
-        const uint32_t j0 = r0 + (blockIdx.x - 1 - nL) * kPanelRows;
+        const uint32_t j0 = r0 + (b - 1 - nL) * kPanelRows;
         const uint32_t ncol = min(uint32_t(kPanelRows), m - j0);
-        for (uint32_t e = tid; e < ncol * kb; e += blockDim.x) {
-            uint32_t cc = e / kb, rr = e - cc * kb;
-            sW[rr * kPW + cc] = ld_cg(val + doff[j0 + cc] + k0 + rr);
-        }
-        __syncthreads();
-        if (tid < ncol) {
-            float *w = sW + tid;
-            for (uint32_t rr = 0; rr < kb; ++rr) {
-                const float u = w[rr * kPW];
-                for (uint32_t i = rr + 1; i < kb; ++i) w[i * kPW] -= sF[rr * LD + i] * u;
-            }
-        }
-        __syncthreads();
-        for (uint32_t e = tid; e < ncol * kb; e += blockDim.x) {
-            uint32_t cc = e / kb, rr = e - cc * kb;
+        for (uint32_t e = tid; e < ncol * kb; e += kTriThreads) {
+            const uint32_t cc = e / kb, rr = e - cc * kb;
             st_cg(val + doff[j0 + cc] + k0 + rr, sW[rr * kPW + cc]);
         }
     }
@@ -366,11 +260,8 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
     uint32_t nL = (rest + kPanelRows - 1) / kPanelRows;
     uint32_t nU = nL;
     dim3 grid(1 + nL + nU, 1, count);
-    if (kb == uint32_t(kDenseNB))
-        k_dense_panel_full<<<grid, kPanelRows, 0, st>>>(val, stride, doff, m, k0, pert_z, diag_scratch, last_has_l, nL);
-    else
-        k_dense_panel<<<grid, kPanelRows, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
-                                                            last_has_l, nL);
+    k_dense_panel<<<grid, kTriThreads, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
+                                                          last_has_l, nL);
     return cudaGetLastError();
 }
 

@@ -24,12 +24,20 @@
 // column order (fused multiply-add instead of multiply and subtract).
 #include "glu_common.cuh"
 #include "glu_kernels.h"
+#include "glu_tri.cuh"
 
 namespace glu {
 
 namespace {
 
 constexpr int kLD = kSnMaxWidth + 1;  // leading dimension of the diagonal block in shared memory
+constexpr int kSnPW = kSnPanelThreads + 1;  // leading dimension of the L21 rows in shared memory
+// panel shared memory: the diagonal block (either layout), plus the rows of
+// L21 in launches with a supernode wider than one chunk
+constexpr size_t kSnPanelSmem = sizeof(float) * kSnMaxWidth * kTriML;
+constexpr size_t kSnPanelSmemWide = kSnPanelSmem + sizeof(float) * kSnMaxWidth * kSnPW;
+static_assert(kSnMaxWidth * kTriML >= kSnMaxWidth * kLD, "either layout fits");
+static_assert(kSnMaxWidth == kTriMax, "supernode width is the triangular block width");
 constexpr int kTile = 64;             // update tile: 64 rows x 64 targets
 constexpr int kTLd = kTile + 4;       // leading dimension of the update operand tiles
 
@@ -63,80 +71,6 @@ __device__ __forceinline__ uint32_t seg_len(const DevPattern &P, uint32_t j, uin
     return lo;
 }
 
-// Factor the w x w diagonal block in place, register resident: 128 threads,
-// thread = (row, half of the columns) holding 32 values; row c is broadcast
-// through shared memory (double buffered, one barrier per column).  Pivot c
-// is perturbed (GESP, numeric.cu:139-140) when its column has an L part:
-// c < w-1, or m > 0.  Step c: L(i,c) = A(i,c) / U(c,c), then
-// A(i,j) -= L(i,c) U(c,j) for j > c, as in the column algorithm.
-__device__ __forceinline__ void sn_diag_regs(const DevPattern &P, float *__restrict__ val, const Sn &d, float pert,
-                                             float (*urow)[kSnMaxWidth], uint32_t *sBase) {
-    const uint32_t tid = threadIdx.x, lane = tid & 31;
-    const uint32_t row = tid >> 1, half = tid & 1;
-    const uint32_t w = d.w;
-    const bool rv = row < w;
-    if (tid < w) sBase[tid] = P.diag[d.s + tid] - tid;  // position of row s in column s + tid
-    __syncthreads();
-    float a[32];
-#pragma unroll
-    for (int jj = 0; jj < 32; ++jj) {
-        const uint32_t cc = half * 32 + jj;
-        a[jj] = (rv && cc < w) ? ld_cg(val + sBase[cc] + row) : 0.0f;
-    }
-#pragma unroll
-    for (int c = 0; c < int(kSnMaxWidth); ++c) {
-        if (uint32_t(c) >= w) break;
-        const int hc = c >> 5, jc = c & 31;
-        float *u = urow[c & 1];
-        if (row == uint32_t(c)) {
-            if (half == uint32_t(hc)) {
-                const bool has_l = (uint32_t(c) + 1 < w) || d.m > 0;
-                float p = a[jc];
-                if (has_l && pert > 0.0f && fabsf(p) < pert) p = pert;
-                a[jc] = p;
-            }
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj)
-                if (int(half) * 32 + jj >= c) u[half * 32 + jj] = a[jj];
-        }
-        __syncthreads();
-        const float lsrc = __shfl_sync(0xffffffffu, a[jc], (lane & ~1u) | uint32_t(hc));
-        if (rv && row > uint32_t(c)) {
-            const float l = lsrc / u[c];
-            if (half == uint32_t(hc)) a[jc] = l;
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj)
-                if (int(half) * 32 + jj > c) a[jj] = fmaf(-l, u[half * 32 + jj], a[jj]);
-        }
-    }
-#pragma unroll
-    for (int jj = 0; jj < 32; ++jj) {
-        const uint32_t cc = half * 32 + jj;
-        if (rv && cc < w) st_cg(val + sBase[cc] + row, a[jj]);
-    }
-}
-
-// Row r of L21: x U11 = a (a = row r of A21), W >= w columns in registers.
-template <int W>
-__device__ __forceinline__ void sn_l21_row(float *__restrict__ val, const uint32_t *sOff, uint32_t w, uint32_t r,
-                                           const float *sF) {
-    float a[W];
-#pragma unroll
-    for (int c = 0; c < W; ++c) a[c] = uint32_t(c) < w ? ld_cg(val + sOff[c] + r) : 0.0f;
-#pragma unroll
-    for (int c = 0; c < W; ++c) {
-        if (uint32_t(c) < w) {
-            const float l = a[c] / sF[c * kLD + c];
-            a[c] = l;
-#pragma unroll
-            for (int j = c + 1; j < W; ++j) a[j] = fmaf(-l, sF[j * kLD + c], a[j]);
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < W; ++c)
-        if (uint32_t(c) < w) st_cg(val + sOff[c] + r, a[c]);
-}
-
 // Target column j of U12 by one warp: L11 x = a over the supernode's rows
 // present in column j (a suffix from row z; the rows above it are structural
 // zeros and stay untouched).  Lane k holds rows k and k + 32.
@@ -159,6 +93,62 @@ __device__ __forceinline__ void sn_u12_warp(float *__restrict__ val, const Sn &d
 }
 
 constexpr uint32_t kFull = 0xffffffffu;
+
+// Diagonal block of one narrow supernode (2 <= w <= kSnSmallWidth) by one
+// warp: lane r holds row r; step c broadcasts row c by shuffles.  Same
+// operations as tri_diag_lu: pivot c perturbed (GESP) when its column has an
+// L part (c < w - 1, or m > 0); L(r,c) = A(r,c) / U(c,c), then A(r,j) -=
+// L(r,c) U(c,j) for j > c.
+__device__ __forceinline__ void sn_diag_small(const DevPattern &P, const SnPlanDev &S, float *__restrict__ val,
+                                              uint32_t i, float pert, uint32_t lane) {
+    constexpr int SW = int(kSnSmallWidth);
+    const Sn d = sn_load(S, i);
+    const uint32_t w = d.w;
+    const bool rv = lane < w;
+    const uint32_t bc = rv ? P.diag[d.s + lane] - lane : 0u;  // position of row s in column s + lane
+    float a[SW];
+#pragma unroll
+    for (int c = 0; c < SW; ++c) {
+        const uint32_t b = __shfl_sync(kFull, bc, c);
+        a[c] = (rv && uint32_t(c) < w) ? ld_cg(val + b + lane) : 0.0f;
+    }
+#pragma unroll
+    for (int c = 0; c < SW; ++c) {
+        if (uint32_t(c) >= w) break;
+        if (lane == uint32_t(c)) {
+            const bool has_l = uint32_t(c) + 1 < w || d.m > 0;
+            if (has_l && pert > 0.0f && fabsf(a[c]) < pert) a[c] = pert;
+        }
+        const float piv = __shfl_sync(kFull, a[c], c);
+        const bool below = rv && lane > uint32_t(c);
+        const float l = a[c] / piv;
+#pragma unroll
+        for (int j = c + 1; j < SW; ++j) {
+            const float uj = __shfl_sync(kFull, a[j], c);
+            if (below) a[j] = fmaf(-l, uj, a[j]);
+        }
+        if (below) a[c] = l;
+    }
+#pragma unroll
+    for (int c = 0; c < SW; ++c) {
+        const uint32_t b = __shfl_sync(kFull, bc, c);
+        if (rv && uint32_t(c) < w) st_cg(val + b + lane, a[c]);
+    }
+}
+
+// Row r of L21 for a supernode of width w <= N <= kTriChunk: x U11 = a in
+// registers (U11 row-major in sM).
+template <int N>
+__device__ __forceinline__ void sn_l21_chunk(float *__restrict__ val, const uint32_t *sOff, uint32_t w, uint32_t r,
+                                             const float *sM) {
+    float x[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) x[c] = uint32_t(c) < w ? ld_cg(val + sOff[c] + r) : 0.0f;
+    tri_chunk_solve<true>(x, sM, 0, w);
+#pragma unroll
+    for (int c = 0; c < N; ++c)
+        if (uint32_t(c) < w) st_cg(val + sOff[c] + r, x[c]);
+}
 
 // Panel of one small supernode (w <= kSnSmallWidth, m <= 32, nt <= 32) by one
 // warp: lane r solves L21 row r, lane j solves target column j of U12, with
@@ -273,17 +263,42 @@ __device__ __forceinline__ void sn_update_small(const DevPattern &P, const SnPla
 
 }  // namespace
 
-// Diagonal blocks of one level's supernodes [i0, i0 + gridDim.x), factored in
-// place (width-1 supernodes have none).  blockIdx.z selects the value set.
-__global__ void __launch_bounds__(128) k_sn_diag(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
-                                                 const float *pert_z, uint32_t i0) {
-    __shared__ float urow[2][kSnMaxWidth];
+// Diagonal-block launch of one level: blocks [b0, b0 + gridDim.x) of the
+// diagonal map, each one supernode wider than kSnSmallWidth (tri_diag_lu) or
+// up to eight narrower ones (a warp each).  The diagonal block is factored in
+// place: pivot c is perturbed (GESP, numeric.cu:139-140) when its column has
+// an L part (c < w - 1, or m > 0); step c: L(i,c) = A(i,c) / U(c,c), then
+// A(i,j) -= L(i,c) U(c,j) for j > c, as in the column algorithm.  blockIdx.z
+// selects the value set.
+__global__ void __launch_bounds__(kTriThreads, 1) k_sn_diag(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
+                                                            const float *pert_z, uint32_t b0) {
+    __shared__ __align__(16) float urow[2][kTriMax];
     __shared__ uint32_t sBase[kSnMaxWidth];
-    const Sn d = sn_load(S, i0 + blockIdx.x);
-    if (d.w < 2) return;
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
-    sn_diag_regs(P, val, d, pert, urow, sBase);
+    const uint2 bi = S.dmap[b0 + blockIdx.x];
+    if (bi.y & kSnSmallFlag) {
+        const uint32_t wi = threadIdx.x >> 5;
+        if (wi < (bi.y & ~kSnSmallFlag)) sn_diag_small(P, S, val, S.dsmall[bi.x + wi], pert, threadIdx.x & 31);
+        return;
+    }
+    const Sn d = sn_load(S, bi.x);
+    const uint32_t tid = threadIdx.x, w = d.w;
+    if (tid < w) sBase[tid] = P.diag[d.s + tid] - tid;  // position of row s in column s + tid
+    __syncthreads();
+    const uint32_t row = tid >> 2, q = tid & 3;
+    float a[kTriChunk];
+#pragma unroll
+    for (int jj = 0; jj < kTriChunk; ++jj) {
+        const uint32_t cc = q * kTriChunk + jj;
+        a[jj] = (row < w && cc < w) ? ld_cg(val + sBase[cc] + row) : 0.0f;
+    }
+    tri_diag_lu(a, w, d.m > 0, pert, urow);
+#pragma unroll
+    for (int jj = 0; jj < kTriChunk; ++jj) {
+        const uint32_t cc = q * kTriChunk + jj;
+        if (row < w && cc < w) st_cg(val + sBase[cc] + row, a[jj]);
+    }
 }
 
 // Panel launch of one level (after its diagonal blocks): blocks [b0, b0 +
@@ -291,9 +306,11 @@ __global__ void __launch_bounds__(128) k_sn_diag(DevPattern P, SnPlanDev S, floa
 // thread), then, for width >= 2, ceil(nt / 4) blocks of U12 target columns
 // (one column per warp).  Width 1: the blocks scale the column by its pivot
 // (numeric.cu:133-143).  blockIdx.z selects the value set.
-__global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPlanDev S, float *val_base,
+__global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, SnPlanDev S, float *val_base,
                                                               uint64_t stride, const float *pert_z, uint32_t b0) {
-    __shared__ float sF[kSnMaxWidth * kLD];
+    extern __shared__ float4 snp_sm4[];
+    float *sF = reinterpret_cast<float *>(snp_sm4);  // L11 column-major (U12 blocks) or U11 row-major (L21 blocks)
+    float *sW = sF + kSnMaxWidth * kTriML;           // rows of L21 when w > kTriChunk
     __shared__ uint32_t sOff[kSnMaxWidth];
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
@@ -317,9 +334,13 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
         return;
     }
     const uint32_t w = d.w;
+    const uint32_t nLb = (d.m + kSnPanelThreads - 1) / kSnPanelThreads;
+    const bool lrows = t < nLb;
     if (tid < w) sOff[tid] = P.diag[d.s + tid];
     __syncthreads();
-    // the factored diagonal block, eight independent loads in flight per thread
+    // the factored diagonal block, eight independent loads in flight per thread:
+    // L21 blocks keep U11 row-major (leading dimension kTriML), U12 blocks L11
+    // column-major (leading dimension kLD)
     for (uint32_t e0 = 0; e0 < kSnMaxWidth * kSnMaxWidth; e0 += 8 * kSnPanelThreads) {
         float v[8];
 #pragma unroll
@@ -330,29 +351,38 @@ __global__ void __launch_bounds__(kSnPanelThreads) k_sn_panel(DevPattern P, SnPl
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const uint32_t e = e0 + q * kSnPanelThreads + tid, cc = e >> 6, r = e & 63;
-            if (cc < w && r < w) sF[cc * kLD + r] = v[q];
+            if (cc < w && r < w) {
+                if (lrows)
+                    sF[r * kTriML + cc] = v[q];
+                else
+                    sF[cc * kLD + r] = v[q];
+            }
         }
         if (e0 + 8 * kSnPanelThreads >= w * kSnMaxWidth) break;
     }
     __syncthreads();
-    if (tid < w) sOff[tid] += d.l + 1 - (d.s + tid);
+    if (tid < w) {
+        sOff[tid] += d.l + 1 - (d.s + tid);
+        if (lrows) sF[tid * kTriML + kTriMax] = 1.0f / sF[tid * kTriML + tid];  // pivot reciprocals
+    }
     __syncthreads();
-    const uint32_t nLb = (d.m + kSnPanelThreads - 1) / kSnPanelThreads;
-    if (t < nLb) {
+    if (lrows) {
+        // row r of L21: x U11 = a (a = row r of A21)
         const uint32_t r = t * kSnPanelThreads + tid;
         if (r >= d.m) return;
-        if (w <= 2)
-            sn_l21_row<2>(val, sOff, w, r, sF);
-        else if (w <= 4)
-            sn_l21_row<4>(val, sOff, w, r, sF);
-        else if (w <= 8)
-            sn_l21_row<8>(val, sOff, w, r, sF);
-        else if (w <= 16)
-            sn_l21_row<16>(val, sOff, w, r, sF);
-        else if (w <= 32)
-            sn_l21_row<32>(val, sOff, w, r, sF);
-        else
-            sn_l21_row<64>(val, sOff, w, r, sF);
+        if (w <= 2) {
+            sn_l21_chunk<2>(val, sOff, w, r, sF);
+        } else if (w <= 4) {
+            sn_l21_chunk<4>(val, sOff, w, r, sF);
+        } else if (w <= 8) {
+            sn_l21_chunk<8>(val, sOff, w, r, sF);
+        } else if (w <= uint32_t(kTriChunk)) {
+            sn_l21_chunk<kTriChunk>(val, sOff, w, r, sF);
+        } else {
+            for (uint32_t c = 0; c < w; ++c) sW[c * kSnPW + tid] = ld_cg(val + sOff[c] + r);
+            tri_rows_solve<true>(sW, kSnPW, tid, sF, w);
+            for (uint32_t c = 0; c < w; ++c) st_cg(val + sOff[c] + r, sW[c * kSnPW + tid]);
+        }
     } else {
         const uint32_t jt = (t - nLb) * (kSnPanelThreads / 32) + tid / 32;
         if (jt < d.nt) {
@@ -537,16 +567,23 @@ __global__ void __launch_bounds__(256) k_sn_positions(DevPattern P, SnPlanDev S,
 }
 
 cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                           const float *pert_z, uint32_t i0, uint32_t i1, cudaStream_t st) {
-    if (i1 <= i0) return cudaSuccess;
-    k_sn_diag<<<dim3(i1 - i0, 1, count), 128, 0, st>>>(P, S, val, stride, pert_z, i0);
+                           const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st) {
+    if (blocks == 0) return cudaSuccess;
+    k_sn_diag<<<dim3(blocks, 1, count), kTriThreads, 0, st>>>(P, S, val, stride, pert_z, b0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                            const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st) {
+                            const float *pert_z, uint32_t b0, uint32_t blocks, uint32_t maxw, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, 0, st>>>(P, S, val, stride, pert_z, b0);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_sn_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSnPanelSmemWide));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const size_t smem = maxw > uint32_t(kTriChunk) ? kSnPanelSmemWide : kSnPanelSmem;
+    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, smem, st>>>(P, S, val, stride, pert_z, b0);
     return cudaGetLastError();
 }
 

@@ -44,12 +44,15 @@ constexpr uint32_t kSnPanelThreads = 128;  // threads of a panel block (rows or 
 
 constexpr uint32_t kSnSmallWidth = 16;         // small supernode: width <= this, few off-diagonal rows/entries
 constexpr uint32_t kSnSmallFlag = 0x80000000u;  // block-map entry of a group of small supernodes
+constexpr uint32_t kSnDiagSmallPerBlock = 8;    // narrow diagonal blocks per block of the diagonal launches (a warp each)
 
 // Supernodes in level order: their records, the block maps of the panel and
 // update launches, the target metadata and the update's position table
 // (nullable) with its offset per supernode.
 struct SnPlanDev {
     const uint4 *meta;        // per supernode: {first column, width, L21 rows m, targets nt}
+    const uint2 *dmap;        // per diagonal-block block: {supernode, 0} or {first of dsmall, kSnSmallFlag | count}
+    const uint32_t *dsmall;   // supernodes of width 2..kSnSmallWidth of the diagonal launches, eight to a block
     const uint2 *pmap;        // per panel block: {supernode, part} or {first of psmall, kSnSmallFlag | count}
     const uint2 *umap;        // per update block: {supernode, tile} or {first of usmall, kSnSmallFlag | count}
     const uint32_t *psmall;   // small supernodes of the panel launches, four to a block
@@ -60,12 +63,12 @@ struct SnPlanDev {
     const uint64_t *pos_off;  // [count]
 };
 
-// Supernodes [i0, i1) of one level (diag); blocks [b0, b0 + blocks) of the
-// panel or update map.  diag runs before panel, panel before update.
+// Blocks [b0, b0 + blocks) of one level's diagonal-block, panel or update
+// map.  diag runs before panel, panel before update.
 cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                           const float *pert_z, uint32_t i0, uint32_t i1, cudaStream_t st);
+                           const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st);
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                            const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st);
+                            const float *pert_z, uint32_t b0, uint32_t blocks, uint32_t max_width, cudaStream_t st);
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                              uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st);
 // Setup, once per pattern: the target metadata (S.meta, S.tgt_off set), then
