@@ -12,8 +12,10 @@
 //              registers), L21 = A21 U11^-1, U12 = L11^-1 A12;
 //   2. update: A22 -= L21 U12 (register-tiled FP32).
 // Each entry receives the same operations as in the column algorithm (FP32,
-// different summation order).  GESP perturbation (numeric.cu:139-140) is
-// applied to every pivot whose column has an L part.
+// different summation order; L21 entries are multiplied by the pivot's
+// correctly rounded reciprocal instead of divided by the pivot).  GESP
+// perturbation (numeric.cu:139-140) is applied to every pivot whose column
+// has an L part.
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 #include "glu_tri.cuh"

@@ -21,7 +21,9 @@
 //           column j (a position table built once per pattern, or a search in
 //           column j's row list).
 // Every entry receives the operations of the column algorithm in the same
-// column order (fused multiply-add instead of multiply and subtract).
+// column order (fused multiply-add instead of multiply and subtract; the L21
+// rows of supernodes wider than one are multiplied by the pivot's correctly
+// rounded reciprocal instead of divided by the pivot).
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 #include "glu_tri.cuh"
