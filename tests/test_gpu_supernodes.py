@@ -2,9 +2,11 @@
 
 The supernodal path groups runs of columns with nested lower patterns and a
 dense diagonal block (widths 1..64) and levels them by the reference's column
-dependencies.  Every width limit, with and without the dense trailing block,
-must reproduce the oracle's FP32 column algorithm (src/numeric.cu) within the
-factor tolerance: per-column max-relative difference <= 1e-4.
+dependencies.  Every width limit (20 and 40 end inside a 16-column chunk of
+the diagonal-block LU and the row solves), with and without the dense
+trailing block, must reproduce the oracle's FP32 column algorithm
+(src/numeric.cu) within the factor tolerance: per-column max-relative
+difference <= 1e-4.
 """
 import numpy as np
 import pytest
@@ -56,7 +58,7 @@ def _reference(lu, perturb=False):
 
 
 @pytest.mark.parametrize("name", ["config0", "mesh90", "nodal2500"])
-@pytest.mark.parametrize("width", [0, 1, 3, 64])
+@pytest.mark.parametrize("width", [0, 1, 3, 20, 40, 64])
 @pytest.mark.parametrize("tail", ["tail", "notail"])
 def test_supernode_width_matches_oracle(name, width, tail):
     A = _matrix(name)
