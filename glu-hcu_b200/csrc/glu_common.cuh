@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 namespace glu {
 
 // Device copy of the L+U pattern (Symbolic_Matrix arrays plus csr_pos).
@@ -25,6 +27,29 @@ enum : uint32_t {
     DEV_NONFINITE_PIVOT = 2u,
     DEV_TIMEOUT = 4u,
     DEV_BAD_INDEX = 8u,
+};
+
+// Runs a setup step (a kernel attribute: dynamic shared memory above 48 KB, a
+// non-portable cluster size) once per device.  Function attributes belong to
+// the device that was current when they were set, and launchers run on the
+// device of their handle, from any host thread.
+class PerDeviceOnce {
+  public:
+    template <class F>
+    cudaError_t run(F &&setup) {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return setup();
+        const uint64_t bit = uint64_t(1) << dev;
+        if (done_.load(std::memory_order_acquire) & bit) return cudaSuccess;
+        e = setup();
+        if (e == cudaSuccess) done_.fetch_or(bit, std::memory_order_acq_rel);
+        return e;
+    }
+
+  private:
+    std::atomic<uint64_t> done_{0};
 };
 
 // Upper bound on spins of any device-side wait before it gives up and

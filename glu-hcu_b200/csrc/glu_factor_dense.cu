@@ -251,13 +251,11 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
 cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
                                float *diag_scratch, uint32_t last_has_l, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_dense_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(kPanelSmem));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_dense_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPanelSmem));
+    });
+    if (e != cudaSuccess) return e;
     uint32_t rest = m - (k0 + kb);
     uint32_t nL = (rest + kPanelRows - 1) / kPanelRows;
     uint32_t nU = nL;
@@ -270,16 +268,16 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
 cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
                                 DenseRegion reg, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_dense_update<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    static PerDeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        cudaError_t r = cudaFuncSetAttribute(k_dense_update<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              int(UpdateTile<128>::Smem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_dense_update<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (r == cudaSuccess)
+            r = cudaFuncSetAttribute(k_dense_update<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(UpdateTile<64>::Smem));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+        return r;
+    });
+    if (e != cudaSuccess) return e;
     const uint32_t rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
     const uint32_t cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
     if ((rows == 0 || cols == 0) && !reg.writeback) return cudaSuccess;

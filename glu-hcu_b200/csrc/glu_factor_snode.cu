@@ -578,12 +578,11 @@ cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, 
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                             const float *pert_z, uint32_t b0, uint32_t blocks, uint32_t maxw, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_sn_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSnPanelSmemWide));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_sn_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSnPanelSmemWide));
+    });
+    if (e != cudaSuccess) return e;
     const size_t smem = maxw > uint32_t(kTriChunk) ? kSnPanelSmemWide : kSnPanelSmem;
     k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, smem, st>>>(P, S, val, stride, pert_z, b0);
     return cudaGetLastError();

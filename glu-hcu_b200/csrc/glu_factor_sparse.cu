@@ -201,11 +201,11 @@ cudaError_t launch_scale_level(const DevPattern &P, const FactorPlanDev &F, floa
 cudaError_t launch_factor_chain(const DevPattern &P, const FactorPlanDev &F, float *val,
                                 uint64_t stride, uint32_t count, const float *pert_z, uint32_t l0,
                                 uint32_t l1, uint32_t cluster, cudaStream_t st) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_factor_chain, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        attr_set = true;
-    }
+    static PerDeviceOnce cluster_attr;
+    cudaError_t e = cluster_attr.run([] {
+        return cudaFuncSetAttribute(k_factor_chain, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    });
+    if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster, 1, count);
     cfg.blockDim = dim3(kChainThreads, 1, 1);
