@@ -118,6 +118,8 @@ class Clocks:
 
 
 def dist_setup(args):
+    """One process per GPU (torchrun env); NCCL, or gloo on a host without GPUs
+    (the reference arm's CPU ranks)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -125,21 +127,33 @@ def dist_setup(args):
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
 
 def max_over_ranks(x, pg, device):
+    """The maximum of x over all ranks (a device tensor under NCCL, a host
+    tensor under gloo)."""
     if pg is None:
         return x
     import torch
 
+    if pg.get_backend() != "nccl":
+        device = "cpu"
     t = torch.tensor([x], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(world, solves_per_rank, ms_max):
+    """Solves per second of the whole job: every rank's solves over the
+    slowest rank's time per step."""
+    return world * solves_per_rank / (ms_max / 1e3)
 
 
 def cpu_reference(W, steps, warmup, sample_only=False):
@@ -267,7 +281,9 @@ def main():
         return
     W = workload(args.workload, args.side)
     if args.impl == "reference":
-        if rank != 0:
+        if rank != 0:  # rank 0 alone times the reference; no collective follows
+            if pg:
+                pg.destroy_process_group()
             return
         v, dt, thr, sample, _ = cpu_reference(W, args.steps, args.warmup)
         line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
@@ -278,6 +294,8 @@ def main():
                                  "sample": sample},
                 "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        if pg:
+            pg.destroy_process_group()
         return
 
     import torch
@@ -345,7 +363,7 @@ def main():
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(ms, pg, dev)
     solves = B * nrhs
-    value = world * solves / (ms / 1e3)
+    value = whole_job_value(world, solves, ms)
     residual = rst.residual
     iters = rst.iterations
 
@@ -401,7 +419,7 @@ def main():
         h2d = vals[:B].nbytes + b_host.nbytes
         d2h = b_host.nbytes
     e2e_ms = max_over_ranks(e2e_ms, pg, dev)
-    e2e_value = world * solves / (e2e_ms / 1e3)
+    e2e_value = whole_job_value(world, solves, e2e_ms)
 
     # roofline of the factorization (all its kernels, one launch sequence)
     peaks = {}
