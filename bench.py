@@ -194,7 +194,7 @@ def cpu_reference(W, steps, warmup, sample_only=False):
     return per_step_solves / dt, dt, threads, sample, x_check["x"]
 
 
-def run_uneven(args, world, rank, local):
+def run_uneven(args, world, rank, local, pg):
     """Uneven batch: 64 independent nodal systems of different sizes, each with
     1-64 right-hand sides, refactored and FP64-refined together (UnevenBatch,
     one stream per worker thread, host buffers)."""
@@ -218,15 +218,20 @@ def run_uneven(args, world, rank, local):
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
     t0 = time.perf_counter()
     for i in range(args.steps):
         xs = step(i)
     torch.cuda.synchronize()
     ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if pg:
+        pg.barrier()
+    ms = max_over_ranks(ms, pg, torch.device("cuda", local))
     res = max(st["residual"] for st in ub.last_refine)
     h2d = sum(v[0].nbytes for v in vals) + sum(b.nbytes for b in bs)
     d2h = sum(x.nbytes for x in xs)
-    value = world * solves / (ms / 1e3)
+    value = whole_job_value(world, solves, ms)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -275,7 +280,7 @@ def main():
     args = parse()
     world, rank, local, pg = dist_setup(args)
     if args.workload == "uneven" and args.impl == "ours":
-        run_uneven(args, world, rank, local)
+        run_uneven(args, world, rank, local, pg)
         if pg:
             pg.destroy_process_group()
         return
