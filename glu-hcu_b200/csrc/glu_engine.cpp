@@ -1094,8 +1094,19 @@ glu_status glu_create_from_pattern(int device, uint32_t n, uint32_t nnz, const u
                                    const uint32_t *csr_diag_ptr, uint32_t batch, glu_handle_t *out) {
     if (!sym_c_ptr || !sym_r_idx || !l_col_ptr || !csr_r_ptr || !csr_c_idx || !csr_diag_ptr)
         return set_error(GLU_ERR_ARG, "null pattern array");
-    if (n == 0 || sym_c_ptr[0] != 0 || sym_c_ptr[n] != nnz || csr_r_ptr[n] != nnz)
+    if (n == 0 || sym_c_ptr[0] != 0 || sym_c_ptr[n] != nnz || csr_r_ptr[0] != 0 || csr_r_ptr[n] != nnz)
         return set_error(GLU_ERR_ARG, "inconsistent pattern");
+    // Every pointer array is checked before any array is indexed through it:
+    // the planners and the level kernel read the arrays without bounds checks.
+    for (uint32_t i = 0; i < n; ++i) {
+        if (sym_c_ptr[i] > sym_c_ptr[i + 1]) return set_error(GLU_ERR_ARG, "sym_c_ptr decreases at column %u", i);
+        if (csr_r_ptr[i] > csr_r_ptr[i + 1]) return set_error(GLU_ERR_ARG, "csr_r_ptr decreases at row %u", i);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        if (csr_diag_ptr[i] < csr_r_ptr[i] || csr_diag_ptr[i] >= csr_r_ptr[i + 1] ||
+            csr_c_idx[csr_diag_ptr[i]] != i)
+            return set_error(GLU_ERR_ARG, "invalid diagonal pointer of row %u", i);
+    }
     SymbolicData s;
     s.n = n;
     s.nnz = nnz;
@@ -1106,12 +1117,15 @@ glu_status glu_create_from_pattern(int device, uint32_t n, uint32_t nnz, const u
     s.csr_c_idx.assign(csr_c_idx, csr_c_idx + nnz);
     s.csr_diag_ptr.assign(csr_diag_ptr, csr_diag_ptr + n);
     for (uint32_t i = 0; i < n; ++i) {
-        if (sym_c_ptr[i] > sym_c_ptr[i + 1] || l_col_ptr[i] < sym_c_ptr[i] || l_col_ptr[i] >= sym_c_ptr[i + 1] ||
-            sym_r_idx[l_col_ptr[i]] != i)
+        if (l_col_ptr[i] < sym_c_ptr[i] || l_col_ptr[i] >= sym_c_ptr[i + 1] || sym_r_idx[l_col_ptr[i]] != i)
             return set_error(GLU_ERR_ARG, "invalid diagonal pointer of column %u", i);
+        // rows strictly ascending in every column (the kernels search them)
+        for (uint32_t p = sym_c_ptr[i] + 1; p < sym_c_ptr[i + 1]; ++p)
+            if (sym_r_idx[p] <= sym_r_idx[p - 1])
+                return set_error(GLU_ERR_ARG, "rows of column %u not strictly ascending", i);
     }
     for (uint32_t p = 0; p < nnz; ++p)
-        if (sym_r_idx[p] >= n) return set_error(GLU_ERR_ARG, "row index out of range");
+        if (sym_r_idx[p] >= n || csr_c_idx[p] >= n) return set_error(GLU_ERR_ARG, "row or column index out of range");
     // CSC positions of the CSR entries (rows ascending in every column)
     s.csr_pos.resize(nnz);
     {

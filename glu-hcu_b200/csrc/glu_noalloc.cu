@@ -2,20 +2,26 @@
 // memory.
 //
 // Some hosts of this library may not call cudaMalloc once they are running:
-// a simulator whose device memory is owned and pooled by a framework, a code
-// path that runs while a CUDA graph is being captured (where cudaMalloc is
-// not allowed), or a real-time loop that must not stall in the allocator.
-// glu_solve allocates its working vectors on first use; this variant takes
-// them from a fixed array in device memory that is part of the library
-// itself, so, once the handle exists and is factored, a solve needs no
-// allocation at all.
+// a simulator whose device memory is owned and pooled by a framework (a second
+// allocator would compete with it for the same memory), or a real-time loop
+// that must not stall in the allocator.  glu_solve allocates its working
+// vectors on first use; this variant takes them from a fixed array in device
+// memory that is part of the library itself, so, once the handle exists and
+// is factored, a solve needs no allocation at all.
 //
 // The array below is held by every GPU that loads the library, for the life
 // of the process.  Its size bounds what this entry point accepts:
 // n * nrhs <= kNoAllocMaxValues and a dense trailing block of order
-// m <= 64 * (kNoAllocMaxBlocks - 1).
+// m <= 64 * (kNoAllocMaxBlocks - 1).  The environment variable
+// GLU_NOALLOC_BLOCK_LIMIT, read once, can lower the second bound (to check
+// the rejection path on small matrices); it cannot raise it.
+//
+// The array keeps the last call's contents.  The sweeps reset the block flags
+// and the ticket they wait on at the start of every call; y and xo are fully
+// written before they are read.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "glu_internal.h"
@@ -52,6 +58,16 @@ glu::Status scratch_address(int dev, float **out) {
     return GLU_OK;
 }
 
+// Dense-tail block limit: kNoAllocMaxBlocks, or less when the environment asks.
+uint32_t block_limit() {
+    static const uint32_t lim = [] {
+        const char *e = std::getenv("GLU_NOALLOC_BLOCK_LIMIT");
+        long v = e ? std::strtol(e, nullptr, 10) : 0;
+        return (v > 0 && v < long(kNoAllocMaxBlocks)) ? uint32_t(v) : kNoAllocMaxBlocks;
+    }();
+    return lim;
+}
+
 }  // namespace
 
 extern "C" glu_status glu_solve_noalloc(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
@@ -69,7 +85,7 @@ extern "C" glu_status glu_solve_noalloc(glu_handle_t h, uint32_t inst, uint32_t 
         uint32_t *flags = reinterpret_cast<uint32_t *>(base + 2 * kNoAllocMaxValues);
         uint32_t *ticket = flags + kNoAllocMaxBlocks;
         s = glu::solve_f32_scratch(h, inst, nrhs, b, x, y, xo, flags, ticket, kNoAllocMaxValues,
-                                   kNoAllocMaxBlocks, stream);
+                                   block_limit(), stream);
     }
     if (prev != dev) cudaSetDevice(prev);
     return s;

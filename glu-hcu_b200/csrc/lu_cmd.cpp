@@ -115,6 +115,7 @@ int main(int argc, char **argv) {
     cout << "Symbolic time: " << ms_since(t0) << " ms" << endl;
 
     t0 = chrono::steady_clock::now();
+    const auto t_gpu = t0;  // the reference's "Total GPU time" span starts at device set-up
     glu_handle_t h = nullptr;
     CHECK(glu_create(sym, 0, 1, &h));
     int32_t nlev = 0;
@@ -145,7 +146,10 @@ int main(int argc, char **argv) {
         cerr << "GPU factorization failed: " << glu_last_error() << endl;
         return 2;
     }
-    cout << "Total GPU time: " << st.last_factor_ms << " ms" << endl;
+    // Same span as the reference's (numeric.cu:431-433 to 621-625): device
+    // set-up, uploads and the factorization; then the factorization alone.
+    cout << "Total GPU time: " << ms_since(t_gpu) << " ms" << endl;
+    cout << "Factorization time: " << st.last_factor_ms << " ms" << endl;
 
     vector<double> x(n);
     if (refine) {

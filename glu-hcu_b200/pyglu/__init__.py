@@ -39,39 +39,39 @@ __all__ = ["splu", "spsolve", "GLUFactorization", "BatchedGLU", "UnevenBatch", "
            "GLUError", "SingularMatrixError", "NotConvergedError", "read_mtx"]
 
 
-def _to_csc_arrays(A):
-    """Return (data_f64, indices_i32, indptr_i32, n) from a sparse matrix.
-
-    Same validation and messages as the reference (pyglu/__init__.py:30-63).
-    """
+def _csc_parts(A):
+    """(data, indices, indptr, shape) of a scipy sparse matrix or a CSC tuple."""
+    if isinstance(A, tuple) and len(A) == 4:
+        return A
     if _HAS_SCIPY and _sp.issparse(A):
-        A = A.tocsc()
-        A.sum_duplicates()
-        A.sort_indices()
-        n = A.shape[0]
-        if A.shape[0] != A.shape[1]:
-            raise ValueError(f"Matrix must be square, got shape {A.shape}")
-        data = np.ascontiguousarray(A.data, dtype=np.float64)
-        indices = np.ascontiguousarray(A.indices, dtype=np.int32)
-        indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
-    elif isinstance(A, tuple) and len(A) == 4:
-        data, indices, indptr, shape = A
-        n = shape[0]
-        if shape[0] != shape[1]:
-            raise ValueError(f"Matrix must be square, got shape {shape}")
-        data = np.ascontiguousarray(data, dtype=np.float64)
-        indices = np.ascontiguousarray(indices, dtype=np.int32)
-        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
-    else:
-        raise TypeError(
-            "A must be a scipy sparse matrix or a "
-            "(data, indices, indptr, shape) tuple in CSC format"
-        )
-    if len(indptr) != n + 1:
-        raise ValueError(f"indptr length {len(indptr)} inconsistent with n={n}")
-    if n == 0:
+        M = A.tocsc()  # a copy for any other format; canonicalised below
+        if M is A:
+            M = A.copy()
+        M.sum_duplicates()
+        M.sort_indices()
+        return M.data, M.indices, M.indptr, M.shape
+    raise TypeError("A must be a scipy sparse matrix or a "
+                    "(data, indices, indptr, shape) tuple in CSC format")
+
+
+def _to_csc_arrays(A):
+    """Return (data_f64, indices_i32, indptr_i32, n) of a square sparse matrix.
+
+    Accepts what the reference's pyglu accepts (pyglu/__init__.py:28-63) and
+    raises the same exception types with the same messages, so that callers
+    matching on them keep working.
+    """
+    data, indices, indptr, shape = _csc_parts(A)
+    rows, cols = shape
+    if rows != cols:
+        raise ValueError(f"Matrix must be square, got shape {shape}")
+    arrays = [np.ascontiguousarray(a, dtype=t)
+              for a, t in ((data, np.float64), (indices, np.int32), (indptr, np.int32))]
+    if arrays[2].shape[0] != rows + 1:
+        raise ValueError(f"indptr length {arrays[2].shape[0]} inconsistent with n={rows}")
+    if rows == 0:
         raise ValueError("Matrix dimension must be > 0")
-    return data, indices, indptr, n
+    return arrays[0], arrays[1], arrays[2], rows
 
 
 def _validate(data, indices, indptr, n):
@@ -201,6 +201,21 @@ class _Engine:
             pass
 
 
+def _check_device_tensor(t, name, dtype, numel, device):
+    """The engine reads and writes device pointers as raw arrays: refuse any
+    tensor whose memory is not exactly what the call will touch."""
+    if not _is_cuda_tensor(t):
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if t.device.index != device:
+        raise ValueError(f"{name} is on cuda:{t.device.index}, the factorization on cuda:{device}")
+    if str(t.dtype) != f"torch.{dtype}":
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if t.numel() != numel:
+        raise ValueError(f"{name} must hold {numel} values, got {t.numel()}")
+
+
 def _is_cuda_tensor(x):
     return hasattr(x, "is_cuda") and x.is_cuda
 
@@ -274,6 +289,7 @@ class GLUFactorization:
 
     def refactor_device(self, data, stream=None):
         """Refactorize from a CUDA float64 tensor of values (no host round trip)."""
+        _check_device_tensor(data, "data", "float64", self._an.nnz_a, self._eng.device)
         eng = _capi.engine()
         st = stream if stream is not None else _stream()
         check(eng.glu_load_source_values(self._eng._h, 0, 1, _capi.C.c_void_p(data.data_ptr()),
@@ -283,9 +299,12 @@ class GLUFactorization:
     def solve_device(self, b, x, refine=True, tol=1e-10, maxiter=10, trans="N", stream=None):
         """Solve with CUDA float64 tensors b, x of shape (k, n) (refined) or
         float32 (plain); returns the refinement statistics."""
+        k = b.shape[0] if b.dim() == 2 else 1
+        dtype = "float64" if refine else "float32"
+        _check_device_tensor(b, "b", dtype, k * self.n, self._eng.device)
+        _check_device_tensor(x, "x", dtype, k * self.n, self._eng.device)
         eng = _capi.engine()
         st = stream if stream is not None else _stream()
-        k = b.shape[0] if b.dim() == 2 else 1
         t = 1 if str(trans).upper() in ("T", "H") else 0
         bp = _capi.C.c_void_p(b.data_ptr())
         xp = _capi.C.c_void_p(x.data_ptr())

@@ -36,15 +36,17 @@ class _SparseSolve:
                     ver = lu._adj_version
                     if v.is_cuda:
                         lu.refactor_device(v.contiguous())
-                        bb = b.detach().to(torch.float64).reshape(1, -1).contiguous()
+                        # the solve runs where the values are, whatever b's device
+                        bb = b.detach().to(device=v.device, dtype=torch.float64).reshape(1, -1).contiguous()
                         x = torch.empty_like(bb)
                         lu.solve_device(bb, x, refine=True, tol=tol, maxiter=maxiter)
-                        x = x.reshape(-1)
+                        x = x.reshape(-1).to(dev)
                     else:
                         lu.refactor(v.cpu().numpy())
                         x = torch.from_numpy(
                             lu.solve(b.detach().cpu().numpy(), refine=True, tol=tol, maxiter=maxiter)).to(dev)
                     ctx.lu = lu
+                    ctx.values_device = values.device
                     ctx.ver = ver
                     ctx.tol = tol
                     ctx.maxiter = maxiter
@@ -62,7 +64,8 @@ class _SparseSolve:
                             lu.refactor(v.cpu().numpy())
                         lu._adj_version = ctx.ver
                     g = gx.detach().to(torch.float64)
-                    if g.is_cuda:
+                    if v.is_cuda:
+                        g = g.to(v.device)
                         gg = g.reshape(1, -1).contiguous()
                         lam = torch.empty_like(gg)
                         lu.solve_device(gg, lam, refine=True, tol=ctx.tol, maxiter=ctx.maxiter, trans="T")
@@ -76,7 +79,7 @@ class _SparseSolve:
                                            device=lam.device)
                     xx = x.to(lam.device)
                     gvals = -lam[rows] * xx[cols]
-                    return gvals.to(v.device), lam.to(gx.device), None, None, None
+                    return gvals.to(ctx.values_device), lam.to(gx.device), None, None, None
 
             cls._fn = SparseSolveFunction
         return cls._fn

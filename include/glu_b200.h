@@ -147,18 +147,21 @@ glu_status glu_solve(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *
                      glu_memory where, glu_stream stream);
 /* glu_solve for callers that cannot allocate device memory.  No counterpart in
  * the reference.  glu_solve allocates its working vectors on first use; some
- * hosts may not call cudaMalloc while they run (device memory owned and pooled
- * by a framework, code running during CUDA graph capture, real-time loops that
- * must not stall in the allocator).  This variant takes the working vectors
- * from a fixed array of about 8 MiB that the library keeps in the memory of
- * every GPU that loads it, for the life of the process, and calls no
- * allocating routine.  b and x are device pointers (nrhs x n FP32), the handle
- * must be factored.  Limits: n * nrhs <= 1,048,576 and a dense trailing block
- * of order <= 262,080; larger problems return GLU_ERR_UNSUPPORTED.  The first
- * call on a device looks up that array's device address (once per device), so
- * make the first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (other streams, other handles, other
- * host threads) race and must be serialized by the caller. */
+ * hosts may not call cudaMalloc while they run: a simulator whose device
+ * memory is owned and pooled by a framework (a second allocator would fight
+ * it for memory), or a real-time loop that must not stall in the allocator.
+ * This variant takes the working vectors from a fixed array of about 8 MiB
+ * that the library keeps in the memory of every GPU that loads it, for the
+ * life of the process, and calls no allocating routine.  b and x are device
+ * pointers (nrhs x n FP32), the handle must be factored.  Limits: n * nrhs <=
+ * 1,048,576 and a dense trailing block of order <= 262,080; larger problems
+ * return GLU_ERR_UNSUPPORTED before touching the GPU.  The first call on a
+ * device looks up that array's device address (once per device), so make the
+ * first call before any stream capture.  Like glu_solve, the call waits for
+ * its stream to finish before it returns (it reads the solve's status).  All
+ * calls share the one array and it keeps the last call's contents: calls that
+ * overlap on the GPU (other streams, other handles, other host threads) race
+ * and must be serialized by the caller. */
 glu_status glu_solve_noalloc(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
                              glu_stream stream);
 /* FP32 solve of A^T x = b with the same factors (U^T then L^T sweeps). */
