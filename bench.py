@@ -42,8 +42,11 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="mesh", choices=["mesh", "nodal", "batch", "uneven"])
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--reference-gpu", action="store_true",
-                   help="also time the reference's own numeric.cu (LUonDevice) on the same arrays")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip timing the reference's own numeric.cu (LUonDevice) on the mesh's arrays")
+    p.add_argument("--reference-gpu", action="store_true", help=argparse.SUPPRESS)  # the default now
+    p.add_argument("--no-batch-record", action="store_true",
+                   help="skip the batched same-pattern sub-record of the mesh line")
     p.add_argument("--side", type=int, default=700, help="mesh side (workload mesh)")
     return p.parse_args()
 
@@ -234,8 +237,8 @@ def run_uneven(args, world, rank, local, pg):
     h2d = sum(v[0].nbytes for v in vals) + sum(b.nbytes for b in bs)
     d2h = sum(x.nbytes for x in xs)
     value = whole_job_value(world, solves, ms)
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": nsteps,
+            "warmup": nwarmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "64 nodal systems, n log-uniform in [2,000, 12,000] (the uneven-batch "
                                    "shape at reduced sizes), 1-64 RHS each, refine to 1e-10",
@@ -305,6 +308,45 @@ def main():
             pg.destroy_process_group()
         return
 
+    line = run_ours(args, W, world, rank, local, pg, args.steps, args.warmup, full=True)
+    if rank == 0 and world == 1 and args.workload == "mesh" and not args.no_batch_record:
+        line["batch"] = batch_record(args, world, rank, local, pg)
+    if rank == 0:
+        print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+
+
+def batch_record(args, world, rank, local, pg, steps=2, warmup=1):
+    """The batched same-pattern workload (256 value sets of one n = 20,000
+    pattern, 4 right-hand sides each) at a couple of steps, with the plain
+    per-matrix FP32 form beside it, as a sub-record of the default line."""
+    import gc
+
+    import torch
+
+    gc.collect()
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    try:
+        b = run_ours(args, workload("batch"), world, rank, local, pg, steps, warmup, full=False)
+    except Exception as e:  # pragma: no cover
+        return {"error": str(e)}
+    keep = ("value", "unit", "ms_per_step", "refactor_ms", "solve_refined_ms", "residual", "residual_inf",
+            "refine_iterations", "plain_form", "factor_roofline", "roofline", "gpu_launches")
+    out = {k: b[k] for k in keep if k in b}
+    out.update(steps=steps, warmup=warmup, workload=b["config"]["workload"], config=b["config"],
+               wall_s=time.perf_counter() - t0)
+    gc.collect()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_ours(args, W, world, rank, local, pg, nsteps, nwarmup, full=True):
+    """One workload through our engine: the timed steps (device-resident
+    inputs), then -- with ``full`` -- the end-to-end pass through the public
+    API, the CPU baseline and the reference's numeric.cu.  Returns the JSON
+    line as a dict."""
     import torch
 
     import pyglu
@@ -347,7 +389,7 @@ def main():
         if s not in (0, _capi.GLU_ERR_NOT_CONVERGED):
             _capi.check(s, "refined solve")
 
-    for i in range(args.warmup):
+    for i in range(nwarmup):
         step(i)
     torch.cuda.synchronize()
     if pg:
@@ -358,7 +400,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     fact_ms = []
     ev0.record(stream)
-    for i in range(args.steps):
+    for i in range(nsteps):
         step(i)
         eng.glu_get_stats(handle, _capi.C.byref(st))
         fact_ms.append(st.last_factor_ms)
@@ -367,7 +409,7 @@ def main():
     clk = clocks.stop()
     if pg:
         pg.barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / nsteps
     ms = max_over_ranks(ms, pg, dev)
     solves = B * nrhs
     value = whole_job_value(world, solves, ms)
@@ -397,8 +439,10 @@ def main():
         x_check = d_x[0, 0].double().cpu().numpy().copy()
 
     # e2e through the public API with host buffers
-    e2e_steps = max(1, min(args.steps, 5))
-    if B == 1:
+    e2e_steps = max(1, min(nsteps, 5))
+    if not full:
+        e2e_ms, h2d, d2h = None, 0, 0
+    elif B == 1:
         # one untimed pass: first-call allocations of the host-buffer path
         lu.refactor(vals[0])
         lu.solve(b_host[0].T if nrhs > 1 else b_host[0, 0], refine=True, tol=W["tol"])
@@ -425,8 +469,10 @@ def main():
         e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
         h2d = vals[:B].nbytes + b_host.nbytes
         d2h = b_host.nbytes
-    e2e_ms = max_over_ranks(e2e_ms, pg, dev)
-    e2e_value = whole_job_value(world, solves, e2e_ms)
+    e2e_value = None
+    if e2e_ms is not None:
+        e2e_ms = max_over_ranks(e2e_ms, pg, dev)
+        e2e_value = whole_job_value(world, solves, e2e_ms)
 
     # roofline of the factorization (all its kernels, one launch sequence)
     peaks = {}
@@ -522,8 +568,8 @@ def main():
             "factor_breakdown_ms": {k: round(v[0], 4) for k, v in kt.items() if v[1]},
             "factor_fp32_tflops": flops / (factor_ms / 1e3) / 1e12}
 
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": nsteps,
+            "warmup": nwarmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": W["desc"], "n": n, "nnz_lu": nnz_lu, "batch": B, "nrhs": nrhs,
                        "levels": st.num_lev, "dense_tail": st.dense_tail, "supernodes": st.supernodes,
@@ -535,35 +581,13 @@ def main():
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": roof, "factor_roofline": factor_roof, "solve_roofline": solve_roof,
             "residual_inf": rst.residual_inf,
-            "gpu_launches": int(st.factor_launches) * args.steps, "clocks": clk}
+            "gpu_launches": int(st.factor_launches) * nsteps, "clocks": clk}
     if B > 1:
         line["plain_form"] = plain_form(W, vals, local, nrhs)
         line["plain_form"]["batched_over_plain"] = value / line["plain_form"]["value"]
-    if rank == 0 and world == 1 and B == 1 and args.reference_gpu:
-        # the reference's own numeric.cu (LUonDevice) on the same arrays and values
-        try:
-            import oracle
-
-            if oracle.ref_gpu_available():
-                p = an.pattern()
-                lp, li = lu.levels()
-                placed = np.zeros(an.nnz_lu, np.float32)
-                placed[an.src_slot] = (vals[0] * an.src_scale).astype(np.float32)
-                # keep its n-long scratch columns below 2^32 elements (numeric.cu:44,82,99)
-                keep = 0
-                if n * 8000 > (1 << 31):
-                    keep = (4 << 30) + 12 * an.nnz_lu + (64 << 20) + 8000 * 4 * n
-                ref_ms = []
-                t0 = time.perf_counter()
-                _, rms = oracle.ref_luondevice(p, placed, lp, li, keep_free_bytes=keep)
-                ref_ms.append(rms)
-                line["reference_numeric_cu"] = {
-                    "total_gpu_ms": ref_ms[-1], "includes": "its allocations, copies in and out (numeric.cu:431-625)",
-                    "wall_ms": (time.perf_counter() - t0) * 1e3, "ballast_free_bytes": keep,
-                    "ours_refactor_ms": factor_ms}
-        except Exception as e:  # pragma: no cover
-            line["reference_numeric_cu"] = {"error": str(e)}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if full and rank == 0 and world == 1 and B == 1 and not args.no_reference_gpu:
+        line["reference_numeric_cu"] = reference_numeric_cu(an, lu, vals[0], n, factor_ms)
+    if full and rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             import oracle
 
@@ -581,10 +605,49 @@ def main():
                         "rel_inf": float(np.abs(dx).max() / np.abs(x_ref).max())}
         except Exception as e:  # pragma: no cover
             line["cpu_baseline"] = {"error": str(e)}
-    if rank == 0:
-        print(json.dumps(line))
-    if pg:
-        pg.destroy_process_group()
+    return line
+
+
+def reference_numeric_cu(an, lu, val0, n, ours_refactor_ms):
+    """The reference's own numeric.cu (LUonDevice, built for sm_100a from the
+    reference tree) on the same arrays and values: its "Total GPU time"
+    (allocations, copies in and out, factorization: numeric.cu:431-625), the
+    span of the same allocations and copies alone, and their difference, the
+    factorization alone."""
+    try:
+        import oracle
+
+        if not oracle.ref_gpu_available():
+            return {"unavailable": "oracle/_ref/libglu_ref_gpu.so not built"}
+        p = an.pattern()
+        lp, li = lu.levels()
+        placed = np.zeros(an.nnz_lu, np.float32)
+        placed[an.src_slot] = (val0 * an.src_scale).astype(np.float32)
+        # keep its n-long scratch columns below 2^32 elements (numeric.cu:44,82,99)
+        keep = 0
+        if n * 8000 > (1 << 31):
+            keep = (4 << 30) + 12 * an.nnz_lu + (64 << 20) + 8000 * 4 * n
+        t0 = time.perf_counter()
+        copy = []
+        ref_val, total = oracle.ref_luondevice(p, placed, lp, li, keep_free_bytes=keep, copy_span=copy)
+        wall = (time.perf_counter() - t0) * 1e3
+        ours = lu.lu_values()
+        cp = p["sym_c_ptr"].astype(np.int64)
+        d = np.abs(ours.astype(np.float64) - ref_val)
+        starts = cp[:-1][np.diff(cp) > 0]
+        rel = np.maximum.reduceat(d, starts) / np.maximum(np.maximum.reduceat(np.abs(ref_val.astype(np.float64)),
+                                                                              starts), 1e-300)
+        factor_only = total - copy[0]
+        return {"total_gpu_ms": total, "copy_span_ms": copy[0], "factor_only_ms": factor_only,
+                "includes": "total: its allocations, copies in and out and the factorization (numeric.cu:431-625); "
+                            "factor_only: total minus the same allocations and copies timed alone",
+                "wall_ms": wall, "ballast_free_bytes": keep, "ours_refactor_ms": ours_refactor_ms,
+                "speedup_vs_factor_only": factor_only / ours_refactor_ms,
+                "speedup_vs_total": total / ours_refactor_ms,
+                "factor_col_max_rel_vs_ours": float(rel.max()),
+                "note": "ours: the value set of the last profiled factorization is value set 0 of the workload"}
+    except Exception as e:  # pragma: no cover
+        return {"error": str(e)}
 
 
 if __name__ == "__main__":

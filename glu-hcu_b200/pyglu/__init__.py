@@ -458,6 +458,14 @@ class UnevenBatch:
     def __len__(self):
         return len(self.lus)
 
+    def analysis(self, i):
+        """The NICSLU preprocessing and symbolic phase of system i."""
+        return self.lus[i].analysis
+
+    def lu_values(self, i):
+        """FP32 factor values of system i (Symbolic_Matrix::val layout)."""
+        return self.lus[i].lu_values()
+
     def _run(self, fn):
         import concurrent.futures as cf
 

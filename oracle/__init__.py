@@ -312,17 +312,22 @@ def _load_ref_gpu():
         lib.ref_gpu_luondevice.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.POINTER(C.c_float), C.c_char_p,
                                            C.c_int]
         lib.ref_gpu_luondevice.restype = C.c_int
+        lib.ref_gpu_copy_span.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_float)]
+        lib.ref_gpu_copy_span.restype = C.c_int
         _refgpu = lib
     return _refgpu
 
 
-def ref_luondevice(pattern, val, level_ptr, level_idx, perturb=False, keep_free_bytes=0):
+def ref_luondevice(pattern, val, level_ptr, level_idx, perturb=False, keep_free_bytes=0, copy_span=None):
     """Run the reference's LUonDevice on the given Symbolic_Matrix arrays.
 
     Returns (factor values, the reference's own "Total GPU time" in ms, which
     includes its allocations and copies).  keep_free_bytes > 0 holds a ballast
     allocation so that only that much device memory is free during the call
-    (bounds the scratch the reference sizes from free memory).
+    (bounds the scratch the reference sizes from free memory).  With
+    ``copy_span`` a list, the span of the same allocations and copies without
+    the factorization (ref_gpu_copy_span) is measured afterwards, with the same
+    ballast, and appended to it in ms.
     """
     lib = _load_ref_gpu()
     ref = _load_ref()
@@ -344,6 +349,11 @@ def ref_luondevice(pattern, val, level_ptr, level_idx, perturb=False, keep_free_
             raise RuntimeError(f"reference LUonDevice failed: {err.value.decode(errors='replace')}")
         out = np.empty(nnz, np.float32)
         ref.ref_get_val(h, out)
+        if copy_span is not None:
+            cs = C.c_float(0)
+            if lib.ref_gpu_copy_span(h, int(keep_free_bytes), C.byref(cs)) != 0:
+                raise RuntimeError("reference copy span failed")
+            copy_span.append(float(cs.value))
         return out, float(ms.value)
     finally:
         ref.ref_destroy(h)

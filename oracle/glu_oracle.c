@@ -19,54 +19,147 @@
  *  orc_leveling -- src/symbolic.cc:106-151.
  *  orc_fill_in -- src/symbolic.cc:11-53.
  */
+#define _GNU_SOURCE /* pthread_barrier_t, sysconf */
 #include "glu_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
-#define FACTOR_BODY(T, FABS)                                                                  \
-    T *tmp = (T *)calloc(n ? n : 1, sizeof(T));                                               \
-    for (int32_t lv = 0; lv < num_lev; ++lv) {                                                \
-        for (int32_t q = level_ptr[lv]; q < level_ptr[lv + 1]; ++q) {                         \
-            uint32_t k = (uint32_t)level_idx[q];                                              \
-            uint32_t dk = diag[k], l0 = dk + 1, l1 = cptr[k + 1];                            \
-            if (l1 == l0) continue;                                                           \
-            if (pert > 0 && FABS(val[dk]) < pert) val[dk] = pert;                             \
-            for (uint32_t p = l0; p < l1; ++p) {                                              \
-                val[p] /= val[dk];                                                            \
-                tmp[ridx[p]] = val[p];                                                        \
+/* The targets j of U-row k are independent (each touches only column j), so
+ * for rows with many targets they are split over a team of threads; every
+ * entry still receives its updates one pivot k at a time, in the same order,
+ * so the result does not depend on the thread count.  Rows are ascending in
+ * every column: A(k,j) is found by binary search and the update starts right
+ * after it, skipping the rows <= k that numeric.cu:58-89 scans without
+ * changing them. */
+#define FACTOR_UPDATE(T)                                                                      \
+    static void update_targets_##T(const struct fctx_##T *c, uint32_t k, int64_t e0,         \
+                                   int64_t e1) {                                              \
+        for (int64_t e = e0; e < e1; ++e) {                                                   \
+            uint32_t j = c->cidx[e];                                                          \
+            uint32_t lo = c->cptr[j], hi = c->cptr[j + 1];                                    \
+            while (lo < hi) {                                                                 \
+                uint32_t mid = lo + (hi - lo) / 2;                                            \
+                if (c->ridx[mid] < k) lo = mid + 1; else hi = mid;                            \
             }                                                                                 \
-            for (uint32_t e = rdiag[k] + 1; e < rptr[k + 1]; ++e) {                          \
-                uint32_t j = cidx[e];                                                         \
-                T s = 0;                                                                      \
-                for (uint32_t p = cptr[j]; p < cptr[j + 1]; ++p)                              \
-                    if (ridx[p] == k) s = val[p];                                             \
-                for (uint32_t p = cptr[j]; p < cptr[j + 1]; ++p) {                            \
-                    if (ridx[p] > k) {                                                        \
-                        T prod = tmp[ridx[p]] * s;                                            \
-                        val[p] = val[p] + (-prod);                                            \
-                    }                                                                         \
-                }                                                                             \
+            T s = 0;                                                                          \
+            uint32_t p = lo;                                                                  \
+            if (p < c->cptr[j + 1] && c->ridx[p] == k) s = c->val[p++];                       \
+            for (; p < c->cptr[j + 1]; ++p) {                                                 \
+                T prod = c->tmp[c->ridx[p]] * s;                                              \
+                c->val[p] = c->val[p] + (-prod);                                              \
             }                                                                                 \
-            for (uint32_t p = l0; p < l1; ++p) tmp[ridx[p]] = 0;                              \
         }                                                                                     \
+    }
+
+#define FACTOR_CTX(T)                                                                         \
+    struct fctx_##T {                                                                         \
+        uint32_t n;                                                                           \
+        const uint32_t *cptr, *ridx, *diag, *rptr, *cidx, *rdiag;                             \
+        int32_t num_lev;                                                                      \
+        const int32_t *level_ptr, *level_idx;                                                 \
+        T *val, *tmp, pert;                                                                   \
+        int nthreads;                                                                         \
+        pthread_barrier_t bar;                                                                \
+    };
+
+/* Pivot k's own work: GESP, L(:,k) /= d, scatter into the scratch column. */
+#define FACTOR_PIVOT(T, FABS)                                                                 \
+    static int pivot_##T(struct fctx_##T *c, uint32_t k) {                                    \
+        uint32_t dk = c->diag[k], l0 = dk + 1, l1 = c->cptr[k + 1];                           \
+        if (l1 == l0) return 0;                                                               \
+        if (c->pert > 0 && FABS(c->val[dk]) < c->pert) c->val[dk] = c->pert;                  \
+        for (uint32_t p = l0; p < l1; ++p) {                                                  \
+            c->val[p] /= c->val[dk];                                                          \
+            c->tmp[c->ridx[p]] = c->val[p];                                                   \
+        }                                                                                     \
+        return 1;                                                                             \
     }                                                                                         \
-    free(tmp);
+    static void clear_##T(struct fctx_##T *c, uint32_t k) {                                   \
+        for (uint32_t p = c->diag[k] + 1; p < c->cptr[k + 1]; ++p) c->tmp[c->ridx[p]] = 0;   \
+    }
 
-void orc_factor_f32(uint32_t n, const uint32_t *cptr, const uint32_t *ridx, const uint32_t *diag,
-                    const uint32_t *rptr, const uint32_t *cidx, const uint32_t *rdiag,
-                    int32_t num_lev, const int32_t *level_ptr, const int32_t *level_idx, float *val,
-                    float pert) {
-    FACTOR_BODY(float, fabsf)
+#define WIDE_ROW 64 /* targets from which a row is split over the team */
+
+/* Worker w of the team: all workers walk the same pivot sequence; worker 0
+ * does the per-pivot serial work and the narrow rows alone, wide rows are
+ * split between two barriers. */
+#define FACTOR_WORKER(T)                                                                      \
+    struct warg_##T { struct fctx_##T *c; int w; };                                           \
+    static void *worker_##T(void *arg) {                                                      \
+        struct fctx_##T *c = ((struct warg_##T *)arg)->c;                                     \
+        const int w = ((struct warg_##T *)arg)->w, nt = c->nthreads;                          \
+        for (int32_t lv = 0; lv < c->num_lev; ++lv) {                                         \
+            for (int32_t q = c->level_ptr[lv]; q < c->level_ptr[lv + 1]; ++q) {               \
+                uint32_t k = (uint32_t)c->level_idx[q];                                       \
+                if (c->diag[k] + 1 == c->cptr[k + 1]) continue;                               \
+                const int64_t e0 = (int64_t)c->rdiag[k] + 1, e1 = (int64_t)c->rptr[k + 1];    \
+                if (e1 - e0 < WIDE_ROW || nt == 1) {                                          \
+                    if (w == 0) {                                                             \
+                        pivot_##T(c, k);                                                      \
+                        update_targets_##T(c, k, e0, e1);                                     \
+                        clear_##T(c, k);                                                      \
+                    }                                                                         \
+                    continue;                                                                 \
+                }                                                                             \
+                if (w == 0) pivot_##T(c, k);                                                  \
+                pthread_barrier_wait(&c->bar);                                                \
+                const int64_t len = e1 - e0;                                                  \
+                update_targets_##T(c, k, e0 + len * w / nt, e0 + len * (w + 1) / nt);          \
+                pthread_barrier_wait(&c->bar);                                                \
+                if (w == 0) clear_##T(c, k);                                                  \
+            }                                                                                 \
+        }                                                                                     \
+        return NULL;                                                                          \
+    }
+
+#define FACTOR_DEF(T, FABS, NAME)                                                             \
+    FACTOR_CTX(T)                                                                             \
+    FACTOR_UPDATE(T)                                                                          \
+    FACTOR_PIVOT(T, FABS)                                                                     \
+    FACTOR_WORKER(T)                                                                          \
+    void NAME(uint32_t n, const uint32_t *cptr, const uint32_t *ridx, const uint32_t *diag,   \
+              const uint32_t *rptr, const uint32_t *cidx, const uint32_t *rdiag,              \
+              int32_t num_lev, const int32_t *level_ptr, const int32_t *level_idx, T *val,    \
+              T pert) {                                                                       \
+        struct fctx_##T c = {n, cptr, ridx, diag, rptr, cidx, rdiag, num_lev, level_ptr,      \
+                             level_idx, val, NULL, pert, oracle_threads()};                   \
+        c.tmp = (T *)calloc(n ? n : 1, sizeof(T));                                            \
+        pthread_t th[64];                                                                     \
+        struct warg_##T args[64];                                                             \
+        int started = 1;                                                                      \
+        pthread_barrier_init(&c.bar, NULL, (unsigned)c.nthreads);                             \
+        for (int w = 1; w < c.nthreads; ++w) {                                                \
+            args[w].c = &c;                                                                   \
+            args[w].w = w;                                                                    \
+            if (pthread_create(&th[w], NULL, worker_##T, &args[w]) != 0) abort();             \
+            ++started;                                                                        \
+        }                                                                                     \
+        args[0].c = &c;                                                                       \
+        args[0].w = 0;                                                                        \
+        worker_##T(&args[0]);                                                                 \
+        for (int w = 1; w < started; ++w) pthread_join(th[w], NULL);                          \
+        pthread_barrier_destroy(&c.bar);                                                      \
+        free(c.tmp);                                                                          \
+    }
+
+/* Threads of the factorization team: GLU_ORACLE_THREADS, else the online
+ * processors, at most 64. */
+static int oracle_threads(void) {
+    const char *e = getenv("GLU_ORACLE_THREADS");
+    long v = e ? strtol(e, NULL, 10) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (v < 1) v = 1;
+    if (v > 64) v = 64;
+    return (int)v;
 }
 
-void orc_factor_f64(uint32_t n, const uint32_t *cptr, const uint32_t *ridx, const uint32_t *diag,
-                    const uint32_t *rptr, const uint32_t *cidx, const uint32_t *rdiag,
-                    int32_t num_lev, const int32_t *level_ptr, const int32_t *level_idx, double *val,
-                    double pert) {
-    FACTOR_BODY(double, fabs)
-}
+typedef float f32_t;
+typedef double f64_t;
+FACTOR_DEF(f32_t, fabsf, orc_factor_f32)
+FACTOR_DEF(f64_t, fabs, orc_factor_f64)
 
 float orc_pert(uint32_t n, const uint32_t *cptr, const float *val) {
     float norm = 0;

@@ -89,4 +89,65 @@ int ref_gpu_luondevice(RefCtx *c, int perturb, size_t keep_free_bytes, float *to
     return 0;
 }
 
+// The part of LUonDevice's "Total GPU time" that is not factorization: the
+// same allocations and copies (numeric.cu:435-488: eight pattern and value
+// arrays, sixteen streams, the TMPMEMNUM x n scratch sized by the same rule
+// from the free memory and cleared, numeric.cu:618-619: the values copied
+// back, then the frees), timed the same way with the same ballast.  The
+// factorization alone is the total minus this span.  Returns 0, or 2/3 as
+// ref_gpu_luondevice.
+int ref_gpu_copy_span(RefCtx *c, size_t keep_free_bytes, float *span_ms) {
+    void *ballast = nullptr;
+    if (keep_free_bytes > 0) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        if (free_b > keep_free_bytes && cudaMalloc(&ballast, free_b - keep_free_bytes) != cudaSuccess) return 2;
+    }
+    Symbolic_Matrix *s = ref_symbolic_matrix(c);
+    const size_t n = s->n, nnz = s->nnz;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    void *d[8] = {};
+    const size_t bytes[8] = {(n + 1) * 4, nnz * 4, nnz * 4, n * 4, (n + 1) * 4, nnz * 4, n * 4, n * 4};
+    const void *src[8] = {s->sym_c_ptr.data(), s->sym_r_idx.data(), s->val.data(), s->l_col_ptr.data(),
+                          s->csr_r_ptr.data(), s->csr_c_idx.data(), s->csr_diag_ptr.data(), s->level_idx.data()};
+    cudaError_t ce = cudaSuccess;
+    for (int i = 0; i < 8 && ce == cudaSuccess; ++i) ce = cudaMalloc(&d[i], bytes[i]);
+    for (int i = 0; i < 8 && ce == cudaSuccess; ++i) ce = cudaMemcpy(d[i], src[i], bytes[i], cudaMemcpyHostToDevice);
+    cudaStream_t streams[16] = {};
+    for (int j = 0; j < 16 && ce == cudaSuccess; ++j) ce = cudaStreamCreate(&streams[j]);
+    void *tmp = nullptr;
+    if (ce == cudaSuccess) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t reserve = size_t(4) << 30;
+        size_t max_tmp = free_b > reserve ? free_b - reserve : free_b / 2;
+        const size_t first = s->level_ptr.size() > 1 ? size_t(s->level_ptr[1] - s->level_ptr[0]) : 1;
+        const size_t per_col = 4 * n;
+        if (max_tmp < per_col) max_tmp = per_col;
+        size_t num = 4 * n * first <= max_tmp ? first : max_tmp / per_col;
+        if (num == 0) num = 1;
+        ce = cudaMalloc(&tmp, num * per_col);
+        if (ce == cudaSuccess) ce = cudaMemset(tmp, 0, num * per_col);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpy(s->val.data(), d[2], nnz * 4, cudaMemcpyDeviceToHost);
+    cudaEventRecord(e1, 0);
+    cudaError_t se = cudaEventSynchronize(e1);
+    if (ce == cudaSuccess) ce = se;
+    float ms = -1.0f;
+    if (ce == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    for (int i = 0; i < 8; ++i)
+        if (d[i]) cudaFree(d[i]);
+    for (int j = 0; j < 16; ++j)
+        if (streams[j]) cudaStreamDestroy(streams[j]);
+    if (tmp) cudaFree(tmp);
+    if (ballast) cudaFree(ballast);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *span_ms = ms;
+    return ce == cudaSuccess ? 0 : 3;
+}
+
 }  // extern "C"

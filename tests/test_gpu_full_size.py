@@ -1,0 +1,76 @@
+"""Factor parity at the benchmark sizes.
+
+* The 700 x 700 power-grid mesh (n = 490,000, 367k supernodes, a ~4k-wide
+  dense tail): our factors against the reference's own numeric.cu
+  (LUonDevice, built for sm_100a from the reference tree) run on the same
+  Symbolic_Matrix arrays and values on this GPU, with a ballast allocation that
+  keeps its n-long scratch below the 32-bit index wrap (numeric.cu:44,82,99).
+* The batched workload's pattern (n = 20,000, a ~9.4k-wide dense tail factored
+  with the panel look-ahead and the 128-wide update tiles): two value sets of a
+  batch against the oracle's FP32 restatement of the column algorithm.
+
+Bar: per-column max-relative difference of the L+U values <= 1e-4
+(max_i |a_i - b_i| / max_i |b_i| over each column), as the other parity tests.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def col_max_rel(a, b, cptr):
+    cptr = np.asarray(cptr, np.int64)
+    d = np.abs(a.astype(np.float64) - b.astype(np.float64))
+    m = np.abs(b.astype(np.float64))
+    starts = cptr[:-1][np.diff(cptr) > 0]
+    dmax = np.maximum.reduceat(d, starts)
+    bmax = np.maximum.reduceat(m, starts)
+    return float(np.where(bmax > 0, dmax / np.where(bmax > 0, bmax, 1), dmax).max())
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="reference numeric.cu not built")
+def test_mesh700_factors_match_reference_numeric_cu():
+    import pyglu
+    from pyglu import synth
+
+    A = synth.config1()
+    n = A[3]
+    lu = pyglu.GLUFactorization(*A)
+    st = lu.stats
+    assert n == 490000 and st["dense_tail"] >= 2048 and st["supernodes"] > 100000
+    p = lu.pattern()
+    lp, li = lu.levels()
+    an = lu.analysis
+    keep = (4 << 30) + 12 * an.nnz_lu + (64 << 20) + 8000 * 4 * n  # TMPMEMNUM <= ~8,000 < 2^32 / n
+    ref, ms = oracle.ref_luondevice(p, an.predict_lu(), lp, li, keep_free_bytes=keep)
+    assert ms > 0
+    err = col_max_rel(lu.lu_values(), ref, p["sym_c_ptr"])
+    assert err <= TOL, err
+
+
+def test_batch_pattern_factors_match_oracle():
+    """Two value sets of the n = 20,000 batched pattern (two, not 256: the
+    oracle's FP32 restatement takes about a minute per set on the host)."""
+    import pyglu
+    from pyglu import _capi, synth
+
+    A = synth.config2_pattern()
+    vals = synth.perturb_values(*A, count=2, seed=7)
+    bl = pyglu.BatchedGLU(A[1], A[2], A[3], vals)
+    st = bl.stats
+    assert st["dense_tail"] >= 8000  # the look-ahead path with 128-wide update tiles
+    an = bl._an
+    p = an.pattern()
+    lp, li = oracle.leveling(p)
+    for z in range(2):
+        placed = np.zeros(an.nnz_lu, np.float32)
+        placed[an.src_slot] = (vals[z] * an.src_scale).astype(np.float32)
+        ref = oracle.factor(p, placed, lp, li, np.float32)
+        v = np.empty(an.nnz_lu, np.float32)
+        _capi.check(_capi.engine().glu_store_lu_values(bl.handle, z, 1, _capi.ptr(v), _capi.GLU_HOST, None))
+        err = col_max_rel(v, ref, p["sym_c_ptr"])
+        assert err <= TOL, (z, err)

@@ -335,7 +335,6 @@ def test_batched_same_pattern():
     A = synth.nodal(1500, seed=12, band=32, n_long=2, unsym_frac=0.1)
     vals = synth.perturb_values(*A, count=5, seed=1)
     bl = pyglu.BatchedGLU(A[1], A[2], A[3], vals)
-    single = pyglu.GLUFactorization(vals[0], A[1], A[2], A[3])
     b = synth.rhs_uniform(A[3], 3, seed=2)
     B = np.broadcast_to(b, (5, 3, A[3])).copy()
     X = bl.solve(B, tol=1e-12, maxiter=30)
@@ -343,15 +342,19 @@ def test_batched_same_pattern():
         M = sp.csc_matrix((vals[i], A[1], A[2]), shape=(A[3], A[3]))
         for k in range(3):
             assert np.linalg.norm(M @ X[i, k] - b[k]) / np.linalg.norm(b[k]) <= REFINE_TOL
-    # set 0 of the batch equals the single factorization of the same values
-    import ctypes as C
-
+    # every value set's factors against the oracle's FP32 column algorithm
     from pyglu import _capi
 
-    z = single.analysis.nnz_lu
-    v0 = np.empty(z, np.float32)
-    _capi.check(_capi.engine().glu_store_lu_values(bl.handle, 0, 1, _capi.ptr(v0), _capi.GLU_HOST, None))
-    assert col_max_rel(v0, single.lu_values(), single.pattern()["sym_c_ptr"]) <= FACTOR_TOL
+    an = bl._an
+    p = an.pattern()
+    lp, li = oracle.leveling(p)
+    for z in (0, 4):
+        placed = np.zeros(an.nnz_lu, np.float32)
+        placed[an.src_slot] = (vals[z] * an.src_scale).astype(np.float32)
+        ref = oracle.factor(p, placed, lp, li, np.float32)
+        vz = np.empty(an.nnz_lu, np.float32)
+        _capi.check(_capi.engine().glu_store_lu_values(bl.handle, z, 1, _capi.ptr(vz), _capi.GLU_HOST, None))
+        assert col_max_rel(vz, ref, p["sym_c_ptr"]) <= FACTOR_TOL, z
 
 
 def test_adjoint_gradient_matches_finite_differences():

@@ -34,23 +34,29 @@ def test_uneven_batch_refined_solves():
     assert all(s["residual"] <= 1e-10 for s in ub.last_refine)
 
 
-def test_uneven_batch_refactor_matches_single_systems():
-    """A refactor keeps each system's ordering and scaling: the same values
-    through a single GLUFactorization refactored the same way give the same
-    factors (within the FP32 factor tolerance)."""
+def test_uneven_batch_refactor_matches_oracle():
+    """A refactor keeps each system's ordering and scaling: every member's
+    factors of its new values agree with the oracle's FP32 column algorithm on
+    the same values placed into the same pattern."""
     import pyglu
     from pyglu import synth
+
+    import oracle
 
     cases = _systems(count=4, seed=5)
     ub = pyglu.UnevenBatch([A for A, _ in cases], workers=3)
     new_vals = [synth.perturb_values(*A, count=1, seed=9)[0] for A, _ in cases]
     ub.refactor(new_vals)
-    for (A, b), lu, v in zip(cases, ub.lus, new_vals):
-        single = pyglu.GLUFactorization(*A)
-        single.refactor(v)
-        a, ref = lu.lu_values().astype(np.float64), single.lu_values().astype(np.float64)
-        cp = lu.pattern()["sym_c_ptr"].astype(np.int64)
+    for i, v in enumerate(new_vals):
+        an = ub.analysis(i)
+        p = an.pattern()
+        lp, li = oracle.leveling(p)
+        placed = np.zeros(an.nnz_lu, np.float32)
+        placed[an.src_slot] = (v * an.src_scale).astype(np.float32)
+        ref = oracle.factor(p, placed, lp, li, np.float32).astype(np.float64)
+        a = ub.lu_values(i).astype(np.float64)
+        cp = p["sym_c_ptr"].astype(np.int64)
         nz = np.diff(cp) > 0
         scale = np.maximum.reduceat(np.abs(ref), cp[:-1][nz])
         err = np.maximum.reduceat(np.abs(a - ref), cp[:-1][nz]) / np.where(scale > 0, scale, 1)
-        assert err.max() <= 1e-4, err.max()
+        assert err.max() <= 1e-4, (i, err.max())
