@@ -252,16 +252,25 @@ def run_uneven(args, world, rank, local, pg):
         print(json.dumps(line))
 
 
-def plain_form(W, vals, local, nrhs):
+def plain_form(W, vals, local, nrhs, tensor_cores=False):
     """The plain unbatched, unrefined FP32 form on the batch's pattern: one
     value set factored alone, then one FP32 solve of its right-hand sides,
-    device-resident, timed per matrix."""
+    device-resident, timed per matrix.  Without ``tensor_cores`` every update
+    is FP32 FMA (the reference's arithmetic); with it the dense tail updates
+    on the tensor cores as in the batched form."""
     import torch
 
     import pyglu
+    from pyglu import _capi
 
     data, indices, indptr, n = W["A"]
     lu = pyglu.GLUFactorization(vals[0], indices, indptr, n, device=local)
+    eng = _capi.engine()
+    tu = _capi.Tuning()
+    _capi.check(eng.glu_get_tuning(lu.handle, _capi.C.byref(tu)))
+    if not tensor_cores:
+        tu.dense_tc_min = 0
+        _capi.check(eng.glu_set_tuning(lu.handle, _capi.C.byref(tu)))
     dev = torch.device("cuda", local)
     d = [torch.tensor(vals[i], dtype=torch.float64, device=dev) for i in range(2)]
     b = torch.tensor(W["b"](n, nrhs, 11), dtype=torch.float32, device=dev)
@@ -277,8 +286,9 @@ def plain_form(W, vals, local, nrhs):
         if i >= 2:
             ts.append(e0.elapsed_time(e1))
     ms = float(np.median(ts))
-    return {"value": nrhs / (ms / 1e3), "unit": "solves/s", "ms_per_matrix": ms,
-            "form": "one value set: FP32 refactor + FP32 solve of its right-hand sides, no refinement"}
+    form = ("one value set: FP32 refactor + FP32 solve of its right-hand sides, no refinement, "
+            + ("dense tail on the tensor cores (3xTF32)" if tensor_cores else "all updates FP32 FMA"))
+    return {"value": nrhs / (ms / 1e3), "unit": "solves/s", "ms_per_matrix": ms, "form": form}
 
 
 def main():
@@ -333,7 +343,7 @@ def batch_record(args, world, rank, local, pg, steps=2, warmup=1):
     except Exception as e:  # pragma: no cover
         return {"error": str(e)}
     keep = ("value", "unit", "ms_per_step", "refactor_ms", "solve_refined_ms", "residual", "residual_inf",
-            "refine_iterations", "plain_form", "factor_roofline", "roofline", "gpu_launches")
+            "refine_iterations", "plain_form", "plain_form_tc", "factor_roofline", "roofline", "gpu_launches")
     out = {k: b[k] for k in keep if k in b}
     out.update(steps=steps, warmup=warmup, workload=b["config"]["workload"], config=b["config"],
                wall_s=time.perf_counter() - t0)
@@ -507,9 +517,11 @@ def run_ours(args, W, world, rank, local, pg, nsteps, nwarmup, full=True):
         upd = float((Lk[:t_s] * Uk[:t_s]).sum())
         dom_bytes = 8.0 * upd * B
         dom_flops = 2.0 * upd * B
-    elif dom == "k_dense_update":
-        dom_bytes = float((8.0 * mp * mp + 2 * 4.0 * 64 * mp).sum()) * B
-        dom_flops = float((2.0 * 64 * mp * mp).sum()) * B
+    elif dom in ("k_dense_update", "k_dense_update_tc"):
+        # C read and written once per launch, the panels' L21 / U12 read once
+        # (the launches the engine made, summed over the value sets)
+        dom_bytes = float(st.dense_update_bytes)
+        dom_flops = float(st.dense_update_flops)
     elif dom == "k_sn_update":
         # L21 and U12 read once, every m x nt output read and written, positions read
         dom_bytes = float(st.sn_update_bytes) * B
@@ -585,6 +597,8 @@ def run_ours(args, W, world, rank, local, pg, nsteps, nwarmup, full=True):
     if B > 1:
         line["plain_form"] = plain_form(W, vals, local, nrhs)
         line["plain_form"]["batched_over_plain"] = value / line["plain_form"]["value"]
+        line["plain_form_tc"] = plain_form(W, vals, local, nrhs, tensor_cores=True)
+        line["plain_form_tc"]["batched_over_plain"] = value / line["plain_form_tc"]["value"]
     if full and rank == 0 and world == 1 and B == 1 and not args.no_reference_gpu:
         line["reference_numeric_cu"] = reference_numeric_cu(an, lu, vals[0], n, factor_ms)
     if full and rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -1,0 +1,481 @@
+// Trailing update of the dense tail on the 5th-generation tensor cores.
+//
+// The blocked dense LU of the trailing block (glu_factor_dense.cu) spends
+// almost all of its flops in A22 -= L21 U12 with K = 64 or 128 (one panel or a
+// pair).  Here that product runs as tcgen05.mma with FP32 accuracy kept by the
+// three-term TF32 split ("3xTF32"): with a = a_hi + a_lo, a_hi = rna_tf32(a),
+// a_lo = rna_tf32(a - a_hi) (and the same for b),
+//     a b ~= a_lo b_hi + a_hi b_lo + a_hi b_hi,
+// accumulated in FP32 in tensor memory.  The dropped a_lo b_lo term and the
+// rounding of a_lo are below 2^-21 relative to |a b|, so each product carries
+// close to FP32 accuracy; the entry is then updated once, c - sum_k l_ik u_kj,
+// instead of once per k as in the FP32 FMA kernel (same bound on the error of
+// a sum of K products; the entries still receive each panel's contribution
+// in panel order).
+//
+// Data flow per update:
+//   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
+//      split into TF32 hi/lo parts, written K-major as rows of 256 floats
+//      (slots 0..127 hi, 128..255 lo; the first panel of a pair fills slots
+//      0..63, the second 64..127) -- the operand layout the MMA reads.
+//   2. k_dense_update_tc, persistent (one CTA per SM), per 128 x 128 tile of
+//      the trailing block:
+//        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 32 FP32
+//                 operand boxes (128-byte swizzle) into a 3-stage ring;
+//        warp 1   MMA issuer: 3 x 4 tcgen05.mma (M = N = 128, K = 8, kind
+//                 tf32) per stage into one of two TMEM accumulators;
+//        warps 2-5 epilogue: load the C tile from HBM into registers while
+//                 the MMAs run, then tcgen05.ld the accumulator, subtract,
+//                 store; the other accumulator takes the next tile's MMAs.
+//      C stays where it lies (element (i, j) at val[doff[j] + i]), so in-place
+//      tails with irregular column offsets need no copy.
+// All waits on mbarriers are bounded (spin_limit polls); a wait that runs out
+// sets DEV_TIMEOUT, every role leaves its loop, the CTA waits for its own
+// copies and MMAs in flight and frees its tensor memory before returning.
+//
+// The reference's counterpart is the per-column Schur update
+// RL_onecol_updateSubmat (src/numeric.cu:270-319).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "glu_common.cuh"
+#include "glu_kernels.h"
+
+namespace glu {
+namespace {
+
+constexpr int kTile = 128;                               // M = N of an update tile
+constexpr int kChunk = 32;                               // K per stage: one 128-byte row of FP32
+constexpr int kStages = 3;
+constexpr uint32_t kOpBytes = kTile * kChunk * 4;        // one operand part of one stage (16 KB)
+constexpr uint32_t kStageBytes = 4 * kOpBytes;           // A hi, A lo, B hi, B lo
+constexpr int kThreads = 192;                            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t kTmemCols = 2 * kTile;                // two FP32 accumulators of 128 columns
+constexpr size_t kBarBytes = 256;
+constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + 1024;  // + alignment slack
+
+// Instruction descriptor of tcgen05.mma kind::tf32: D FP32 (bits 4-5 = 1), A
+// and B TF32 (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at
+// bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(kTile >> 3) << 17) |
+                            (uint32_t(kTile >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor of a K-major operand tile in the canonical
+// 128-byte-swizzled layout written by a TMA box of 32 FP32 x rows: rows of
+// 128 bytes, 8-row groups 1024 bytes apart (stride byte offset), layout type 2
+// (128-byte swizzle) at bits 61-63, descriptor version 1 at bits 46-47.  The
+// leading byte offset is unused for swizzled K-major layouts.
+__device__ __forceinline__ uint64_t kmajor_sw128_desc(uint32_t saddr) {
+    uint64_t d = uint64_t((saddr & 0x3FFFFu) >> 4);
+    d |= uint64_t(1) << 16;
+    d |= uint64_t(1024 >> 4) << 32;
+    d |= uint64_t(1) << 46;
+    d |= uint64_t(2) << 61;
+    return d;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the completion of the phase with the given parity; false when
+// `limit` polls pass first.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y,
+                                            int z) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_addr(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+// Arrives (once) on the mbarrier when every tcgen05 operation this thread has
+// issued so far is complete.
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+struct Tile {
+    uint32_t z, rbase, cbase;
+};
+__device__ __forceinline__ Tile decode_tile(uint32_t t, uint32_t tiles_r, uint32_t tiles_c, const DenseRegion &reg) {
+    const uint32_t per = tiles_r * tiles_c;
+    Tile o;
+    o.z = t / per;
+    const uint32_t rem = t - o.z * per;
+    const uint32_t tr = rem / tiles_c;
+    o.rbase = reg.r_lo + tr * kTile;
+    o.cbase = reg.c_lo + (rem - tr * tiles_c) * kTile;
+    return o;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- pack --
+// Rows [r_start, m) of the panel's L21 (columns k0 .. k0 + kb - 1) and
+// columns [r_start, m) of its U12 (rows k0 .. k0 + kb - 1), split into TF32
+// hi / lo parts: pack[z][i][slot0 + k] = hi, pack[z][i][128 + slot0 + k] = lo
+// for k < 64 (zero for k >= kb).  Blocks [0, nA) take 128 rows of L21 each,
+// the rest 128 columns of U12; blockIdx.z selects the value set.
+__global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ val_base, uint64_t stride,
+                                                    const uint32_t *__restrict__ doff, uint32_t m, uint32_t k0,
+                                                    uint32_t kb, uint32_t slot0, uint32_t r_start, uint32_t nA,
+                                                    float *__restrict__ packA, float *__restrict__ packB) {
+    __shared__ float sT[kDenseNB][kTile + 1];
+    const float *val = val_base + blockIdx.z * stride;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t r = tid >> 1, h = tid & 1;  // writer: row (or column) r, K half h
+    float x[32];
+    float *dst = nullptr;
+    if (blockIdx.x < nA) {
+        const uint32_t row0 = r_start + blockIdx.x * kTile;
+        for (uint32_t e = tid; e < uint32_t(kDenseNB) * kTile; e += blockDim.x) {
+            const uint32_t k = e / kTile, rr = e - k * kTile;
+            sT[k][rr] = (k < kb && row0 + rr < m) ? ld_cg(val + doff[k0 + k] + row0 + rr) : 0.0f;
+        }
+        __syncthreads();
+        if (row0 + r >= m) return;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = sT[h * 32 + i][r];
+        dst = packA + (size_t(blockIdx.z) * m + row0 + r) * 256 + slot0 + h * 32;
+    } else {
+        const uint32_t j = r_start + (blockIdx.x - nA) * kTile + r;
+        if (j >= m) return;
+        const float *src = val + doff[j] + k0 + h * 32;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) x[i] = (h * 32 + i < kb) ? ld_cg(src + i) : 0.0f;
+        dst = packB + (size_t(blockIdx.z) * m + j) * 256 + slot0 + h * 32;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i += 4) {
+        float4 hi, lo;
+        hi.x = tf32_rna(x[i]);
+        hi.y = tf32_rna(x[i + 1]);
+        hi.z = tf32_rna(x[i + 2]);
+        hi.w = tf32_rna(x[i + 3]);
+        lo.x = tf32_rna(x[i] - hi.x);
+        lo.y = tf32_rna(x[i + 1] - hi.y);
+        lo.z = tf32_rna(x[i + 2] - hi.z);
+        lo.w = tf32_rna(x[i + 3] - hi.w);
+        *reinterpret_cast<float4 *>(dst + i) = hi;
+        *reinterpret_cast<float4 *>(dst + 128 + i) = lo;
+    }
+}
+
+// -------------------------------------------------------------- update --
+// Rows [r_lo, r_hi) x columns [c_lo, c_hi) of the trailing block after the
+// panels [k0, k0 + K) (relative to r0 = k0 + K), in 128 x 128 tiles; K =
+// 32 * nchunks (pack slots beyond the panels' width hold zeros).  Entries of
+// a tile outside the region are computed but neither read nor written.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_dense_update_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      float *val_base, uint64_t stride, const uint32_t *__restrict__ doff, uint32_t m, uint32_t r0,
+                      uint32_t nchunks, DenseRegion reg, uint32_t tiles_r, uint32_t tiles_c, uint32_t count,
+                      const float *__restrict__ diag_scratch, uint32_t *status, uint32_t spin_limit) {
+    extern __shared__ uint8_t tc_smem_raw[];
+    uint8_t *smem = tc_smem_raw + ((1024u - (smem_addr(tc_smem_raw) & 1023u)) & 1023u);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * kStageBytes);
+    uint64_t *full = bars;                   // [kStages] stage loaded (TMA bytes)
+    uint64_t *empty = bars + kStages;        // [kStages] stage consumed (MMA commit)
+    uint64_t *acc_full = bars + 2 * kStages;  // [2] accumulator ready (MMA commit)
+    uint64_t *acc_empty = acc_full + 2;       // [2] accumulator read (4 epilogue warps)
+    uint64_t *done = acc_empty + 2;           // all MMAs of this CTA complete
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t total = tiles_r * tiles_c * count;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 4);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
+                const int ya = int(r0 + tl.rbase), yb = int(r0 + tl.cbase), zz = int(tl.z);
+                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g) {
+                    const uint32_t s = g % kStages, ph = (g / kStages) & 1;
+                    if (!mbar_wait(&empty[s], ph ^ 1, spin_limit)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *st = smem + s * kStageBytes;
+                    mbar_arrive_expect_tx(&full[s], kStageBytes);
+                    const int xh = int(kc * kChunk), xl = 128 + xh;
+                    tma_load_3d(st, &mapA, &full[s], xh, ya, zz);
+                    tma_load_3d(st + kOpBytes, &mapA, &full[s], xl, ya, zz);
+                    tma_load_3d(st + 2 * kOpBytes, &mapB, &full[s], xh, yb, zz);
+                    tma_load_3d(st + 3 * kOpBytes, &mapB, &full[s], xl, yb, zz);
+                }
+            }
+            if (!ok) atomicOr(status, DEV_TIMEOUT);
+            // the last load into every stage lands before the CTA may exit
+            for (uint32_t s = 0; s < uint32_t(kStages) && s < g; ++s) {
+                const uint32_t f = s + ((g - 1 - s) / kStages) * kStages;
+                if (!mbar_wait(&full[s], (f / kStages) & 1, spin_limit)) atomicOr(status, DEV_TIMEOUT);
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            uint32_t g = 0, i = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x, ++i) {
+                const uint32_t a = i & 1, aph = (i >> 1) & 1;
+                if (!mbar_wait(&acc_empty[a], aph ^ 1, spin_limit)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + a * kTile;
+                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g) {
+                    const uint32_t s = g % kStages, ph = (g / kStages) & 1;
+                    if (!mbar_wait(&full[s], ph, spin_limit)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t base = smem_addr(smem + s * kStageBytes);
+#pragma unroll
+                    for (uint32_t k8 = 0; k8 < kChunk / 8; ++k8) {
+                        const uint32_t off = k8 * 32;  // 8 TF32 values = 32 bytes along K
+                        const uint64_t ah = kmajor_sw128_desc(base + off);
+                        const uint64_t al = kmajor_sw128_desc(base + kOpBytes + off);
+                        const uint64_t bh = kmajor_sw128_desc(base + 2 * kOpBytes + off);
+                        const uint64_t bl = kmajor_sw128_desc(base + 3 * kOpBytes + off);
+                        tc_mma_tf32(d, al, bh, (kc | k8) != 0);
+                        tc_mma_tf32(d, ah, bl, 1);
+                        tc_mma_tf32(d, ah, bh, 1);
+                    }
+                    tc_commit(&empty[s]);
+                }
+                if (!ok) break;
+                tc_commit(&acc_full[a]);
+            }
+            if (!ok) atomicOr(status, DEV_TIMEOUT);
+            tc_commit(done);
+            if (!mbar_wait(done, 0, spin_limit)) atomicOr(status, DEV_TIMEOUT);
+        }
+    } else {
+        // ------------------------------------------------ epilogue
+        const uint32_t q = warp & 3;           // TMEM lane quarter this warp may access
+        const uint32_t row = q * 32 + lane;    // tile row of this thread
+        if (reg.writeback) {
+            // the factored diagonal block of the panel at wb_k0, kept in
+            // scratch while that panel's blocks still read the original
+            const uint32_t et = threadIdx.x - 64, wk = reg.wb_k0, wb = min(uint32_t(kDenseNB), m - wk);
+            for (uint32_t z = blockIdx.x; z < count; z += gridDim.x) {
+                float *val = val_base + z * stride;
+                const float *ds = diag_scratch + size_t(z) * kDenseNB * kDenseNB;
+                for (uint32_t e = et; e < wb * wb; e += 128) {
+                    const uint32_t c = e / wb, rr = e - c * wb;
+                    st_cg(val + doff[wk + c] + wk + rr, ds[c * kDenseNB + rr]);
+                }
+            }
+        }
+        uint32_t i = 0;
+        for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+            const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
+            const uint32_t a = i & 1, aph = (i >> 1) & 1;
+            float *val = val_base + tl.z * stride;
+            const bool rok = tl.rbase + row < reg.r_hi;
+            const uint32_t grow = r0 + tl.rbase + row;
+            // column offsets of the tile (lane j holds column j of each chunk)
+            uint32_t coff[4];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                const uint32_t col = tl.cbase + cc * 32 + lane;
+                coff[cc] = col < reg.c_hi ? doff[r0 + col] : 0u;
+            }
+            // C tile row into registers while the MMAs run
+            float c[4][32];
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc)
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) {
+                    const uint32_t o = __shfl_sync(0xffffffffu, coff[cc], jj);
+                    const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
+                    c[cc][jj] = ok ? ld_cg(val + o + grow) : 0.0f;
+                }
+            // warp-uniform: the tcgen05.ld below needs the whole warp
+            if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[a], aph, spin_limit))) {
+                if (lane == 0) atomicOr(status, DEV_TIMEOUT);
+                break;
+            }
+            tc_fence_after();
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                float acc[32];
+                tc_ld32(tmem + ((q * 32) << 16) + a * kTile + cc * 32, acc);
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) {
+                    const uint32_t o = __shfl_sync(0xffffffffu, coff[cc], jj);
+                    const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
+                    if (ok) st_cg(val + o + grow, c[cc][jj] - acc[jj]);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[a]);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// ----------------------------------------------------------------- host --
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+}  // namespace
+
+cudaError_t dense_tc_tensor_map(float *pack, uint32_t m, uint32_t batch, CUtensorMap *map) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[3] = {256, m, batch};
+    const cuuint64_t strides[2] = {256 * sizeof(float), cuuint64_t(m) * 256 * sizeof(float)};
+    const cuuint32_t box[3] = {uint32_t(kChunk), uint32_t(kTile), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pack, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count, const uint32_t *doff, uint32_t m,
+                              uint32_t k0, uint32_t kb, uint32_t slot0, float *packA, float *packB,
+                              cudaStream_t st) {
+    const uint32_t r_start = k0 + kb;
+    if (r_start >= m) return cudaSuccess;
+    const uint32_t nA = (m - r_start + kTile - 1) / kTile;
+    k_dense_pack<<<dim3(2 * nA, 1, count), 256, 0, st>>>(val, stride, doff, m, k0, kb, slot0, r_start, nA, packA,
+                                                           packB);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
+                                   uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
+                                   const float *diag_scratch, DenseRegion reg, uint32_t *status,
+                                   uint32_t spin_limit, uint32_t num_sms, cudaStream_t st) {
+    static PerDeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_dense_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
+    });
+    if (e != cudaSuccess) return e;
+    const uint32_t r0 = k0 + kb;
+    const uint32_t rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
+    const uint32_t cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
+    const uint32_t tiles_r = (rows + kTile - 1) / kTile, tiles_c = (cols + kTile - 1) / kTile;
+    const uint64_t total = uint64_t(tiles_r) * tiles_c * count;
+    if (total == 0 && !reg.writeback) return cudaSuccess;
+    if (r0 > m || total > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    uint32_t grid = uint32_t(std::min<uint64_t>(std::max<uint64_t>(total, 1), num_sms));
+    if (reg.writeback) grid = std::max<uint32_t>(grid, std::min<uint32_t>(count, num_sms));
+    const uint32_t nchunks = (kb + kChunk - 1) / kChunk;
+    k_dense_update_tc<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, val, stride, doff, m, r0, nchunks, reg,
+                                                          tiles_r, tiles_c, count, diag_scratch, status, spin_limit);
+    return cudaGetLastError();
+}
+
+}  // namespace glu

@@ -76,12 +76,12 @@ static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
 // Kernel kinds of glu_factor for the optional per-kernel profile.
 enum KernelKind {
     KK_PERT = 0, KK_LEVEL, KK_CHAIN, KK_SCALE, KK_DGATHER, KK_PANEL, KK_UPDATE, KK_DSCATTER, KK_CHECK,
-    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE
+    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE, KK_PACK, KK_UPDATE_TC
 };
 static const char *const kKindNames[GLU_KERNEL_KINDS] = {
     "k_colsum+k_pert_finish", "k_factor_level", "k_factor_chain", "k_scale_level", "k_dense_gather",
     "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_diag", "k_sn_panel",
-    "k_sn_update"};
+    "k_sn_update", "k_dense_pack", "k_dense_update_tc"};
 
 // Events around every launch of one glu_factor call, when enabled.
 struct KernelProfiler {
@@ -206,6 +206,13 @@ struct glu_handle_s {
     // panel-done / rest-done events
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_panel = nullptr, ev_rest = nullptr;
+    // tensor-core dense update: TF32 hi/lo operand packs and their TMA maps
+    // (allocated on the first factorization that uses them)
+    DevBuf d_packA, d_packB;
+    CUtensorMap map_packA{}, map_packB{};
+    uint32_t pack_m = 0;
+    uint32_t num_sms = 148;
+    uint32_t spin_limit = kSpinLimit;
     KernelProfiler prof;
     bool factored = false;
     glu_stats stats{};
@@ -279,6 +286,8 @@ void find_full_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t
 constexpr double kDenseRate = 30e12, kPanelLatency = 20e-6;
 // Default width from which trailing blocks factor with panel look-ahead.
 constexpr uint32_t kLookaheadMin = 3072;
+// Default width from which trailing blocks update on the tensor cores.
+constexpr uint32_t kDenseTcMin = 1024;
 constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
 
 uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
@@ -833,7 +842,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -857,6 +866,11 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_status), 256), "allocate pinned");
     GLU_CUDA(cudaEventCreate(&h->ev0), "event");
     GLU_CUDA(cudaEventCreate(&h->ev1), "event");
+    {
+        int sms = 0;
+        GLU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device attribute");
+        h->num_sms = uint32_t(std::max(sms, 1));
+    }
     {
         int least = 0, greatest = 0;
         GLU_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
@@ -1313,10 +1327,12 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     GLU_CUDA(cudaEventRecord(h->ev0, st), "event");
     KernelProfiler &pf = h->prof;
     pf.used = 0;
+    uint64_t nlaunch = 0;  // kernel launches of this call
 #define GLU_LAUNCH(kind, call, what)                    \
     do {                                                \
         GLU_CUDA(pf.begin(st), "profile event");        \
         GLU_CUDA((call), (what));                       \
+        ++nlaunch;                                      \
         GLU_CUDA(pf.end((kind), st), "profile event");  \
     } while (0)
     if (perturb) {
@@ -1382,16 +1398,54 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_fork, 0), "stream wait");
     }
     const uint32_t nb = kDenseNB;
+    // tensor-core updates for wide trailing blocks; their operand packs are
+    // allocated once per handle
+    const bool tc = h->m && h->tune.dense_tc_min && h->m >= h->tune.dense_tc_min;
+    if (tc && h->pack_m != h->m) {
+        const size_t pack_bytes = sizeof(float) * 256 * size_t(h->m) * h->batch;
+        GLU_CUDA(h->d_packA.alloc(pack_bytes), "allocate tensor-core operand packs");
+        GLU_CUDA(h->d_packB.alloc(pack_bytes), "allocate tensor-core operand packs");
+        GLU_CUDA(dense_tc_tensor_map(h->d_packA.as<float>(), h->m, h->batch, &h->map_packA), "tensor map");
+        GLU_CUDA(dense_tc_tensor_map(h->d_packB.as<float>(), h->m, h->batch, &h->map_packB), "tensor map");
+        h->pack_m = h->m;
+    }
+    uint32_t *dstatus = h->d_status.as<uint32_t>();
+    double upd_bytes = 0, upd_flops = 0;
     auto update = [&](uint32_t k0, uint32_t kb, DenseRegion reg, cudaStream_t s) -> cudaError_t {
+        const double rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
+        const double cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
+        upd_bytes += double(count) * (8.0 * rows * cols + 4.0 * kb * (rows + cols));
+        upd_flops += double(count) * 2.0 * kb * rows * cols;
         cudaError_t e = pf.begin(s);
-        if (e == cudaSuccess) e = launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, reg, s);
-        if (e == cudaSuccess) e = pf.end(KK_UPDATE, s);
+        if (e != cudaSuccess) return e;
+        if (tc) {
+            e = launch_dense_update_tc(h->map_packA, h->map_packB, dbase, dstride, count, doff, h->m, k0, kb, dscr,
+                                       reg, dstatus, h->spin_limit, h->num_sms, s);
+            if (e == cudaSuccess) e = pf.end(KK_UPDATE_TC, s);
+        } else {
+            e = launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, reg, s);
+            if (e == cudaSuccess) e = pf.end(KK_UPDATE, s);
+        }
+        ++nlaunch;
+        return e;
+    };
+    // TF32 hi/lo operands of panel k0 (slot0 0: first of a pair or alone; 64:
+    // second of a pair), on the panel stream
+    auto pack = [&](uint32_t k0, uint32_t kb, uint32_t slot0) -> cudaError_t {
+        if (!tc) return cudaSuccess;
+        cudaError_t e = pf.begin(ps);
+        if (e == cudaSuccess)
+            e = launch_dense_pack(dbase, dstride, count, doff, h->m, k0, kb, slot0, h->d_packA.as<float>(),
+                                  h->d_packB.as<float>(), ps);
+        if (e == cudaSuccess) e = pf.end(KK_PACK, ps);
+        ++nlaunch;
         return e;
     };
     auto panel = [&](uint32_t k0, uint32_t kb) -> cudaError_t {
         cudaError_t e = pf.begin(ps);
         if (e == cudaSuccess) e = launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, ps);
         if (e == cudaSuccess) e = pf.end(KK_PANEL, ps);
+        ++nlaunch;
         return e;
     };
     for (uint32_t k0 = 0; k0 < h->m;) {
@@ -1402,6 +1456,8 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
             GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
             rest_pending = false;
         }
+        // after the previous pair's update, which reads the packs
+        GLU_CUDA(pack(k0, kb0, 0), "factor (dense pack)");
         if (rest0 <= nb || !lookahead) {  // small trailing blocks, last panels: plain steps
             GLU_CUDA(update(k0, kb0, DenseRegion{0, rest0, 0, rest0, 1, k0}, ps), "factor (dense update)");
             k0 += kb0;
@@ -1412,6 +1468,7 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         GLU_CUDA(update(k0, kb0, DenseRegion{0, nb, 0, rest0, 1, k0}, ps), "factor (dense update)");
         GLU_CUDA(update(k0, kb0, DenseRegion{nb, rest0, 0, nb, 0, k0}, ps), "factor (dense update)");
         GLU_CUDA(panel(k1, kb1), "factor (dense panel)");
+        GLU_CUDA(pack(k1, kb1, kDenseNB), "factor (dense pack)");
         const uint32_t rest1 = h->m - (k1 + kb1), kk = kb0 + kb1;
         if (rest1 <= nb) {
             GLU_CUDA(update(k0, kk, DenseRegion{0, rest1, 0, rest1, 1, k1}, ps), "factor (dense update)");
@@ -1445,6 +1502,9 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.last_factor_ms = ms;
+    h->stats.factor_launches = nlaunch;
+    h->stats.dense_update_bytes = upd_bytes;
+    h->stats.dense_update_flops = upd_flops;
     if (perturb) cudaMemcpy(&h->stats.pert, h->d_pert.as<float>() + first, sizeof(float), cudaMemcpyDeviceToHost);
     h->factored = true;
     if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "factorization wait timed out");

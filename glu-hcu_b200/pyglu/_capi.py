@@ -38,7 +38,7 @@ ENGINE_SYMBOLS = [
     "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
     "glu_kernel_kind_name", "glu_measure_fp32_peak",
 ]
-GLU_KERNEL_KINDS = 12
+GLU_KERNEL_KINDS = 14
 PRE_SYMBOLS = [
     "glu_pre_analyze", "glu_pre_n", "glu_pre_nnz", "glu_pre_matrix", "glu_pre_transform",
     "glu_pre_source_map", "glu_pre_destroy", "glu_pre_read_mtx", "glu_pre_free",
@@ -71,14 +71,15 @@ class Stats(C.Structure):
                 ("factor_flops", C.c_double), ("factor_launches", C.c_uint64),
                 ("last_factor_ms", C.c_float), ("pert", C.c_float), ("supernodes", C.c_uint32),
                 ("sn_levels", C.c_uint32), ("sn_update_flops", C.c_double), ("sn_update_bytes", C.c_double),
-                ("sn_panel_bytes", C.c_double), ("sn_sweep_levels", C.c_uint32)]
+                ("sn_panel_bytes", C.c_double), ("sn_sweep_levels", C.c_uint32),
+                ("dense_update_bytes", C.c_double), ("dense_update_flops", C.c_double)]
 
 
 class Tuning(C.Structure):
     _fields_ = [("wide_work", C.c_uint32), ("chain_cluster", C.c_uint32), ("group_lanes", C.c_uint32),
                 ("dense_tail_min", C.c_uint32), ("dense_tail_max", C.c_uint32), ("solve_thin", C.c_uint32),
                 ("solve_cluster", C.c_uint32), ("sn_width", C.c_uint32),
-                ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32)]
+                ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32), ("dense_tc_min", C.c_uint32)]
 
 
 _vp = C.c_void_p

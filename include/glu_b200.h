@@ -195,7 +195,7 @@ typedef struct {
     uint32_t chain_segments;   /* runs of narrow levels run by the cluster kernel */
     uint32_t dense_tail;       /* order of the trailing block factored densely    */
     double factor_flops;       /* sum_k |L_k| + 2 |L_k||U_k|                      */
-    uint64_t factor_launches;  /* kernel launches of one glu_factor call          */
+    uint64_t factor_launches;  /* kernel launches of the last glu_factor call     */
     float last_factor_ms;      /* device time of the last glu_factor call         */
     float pert;                /* perturbation of the last GESP factorization     */
     uint32_t supernodes;       /* supernodes of the sparse part (0: column path)   */
@@ -205,6 +205,10 @@ typedef struct {
                                   m x nt outputs read and written (+ positions)   */
     double sn_panel_bytes;     /* supernode panels: L21, U12 read and written      */
     uint32_t sn_sweep_levels;  /* levels of the supernodal L and U solve sweeps    */
+    double dense_update_bytes; /* last glu_factor call, dense trailing updates:
+                                  C read and written once per launch plus one
+                                  FP32 read of the panels' L21 and U12          */
+    double dense_update_flops; /* and their flops, 2 K per updated entry        */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
 
@@ -214,7 +218,7 @@ glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
  * summed milliseconds and launch counts of the last glu_factor call (arrays
  * of GLU_KERNEL_KINDS entries; see glu_kernel_kind_name).  Off by default:
  * the events add a little time between launches. */
-#define GLU_KERNEL_KINDS 12
+#define GLU_KERNEL_KINDS 14
 glu_status glu_profile_enable(glu_handle_t h, int on);
 glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
 const char *glu_kernel_kind_name(int kind);
@@ -241,6 +245,9 @@ typedef struct {
     uint32_t dense_lookahead;  /* dense trailing blocks at least this wide factor
                                   the next panel during the current update
                                   (0: never)                                     */
+    uint32_t dense_tc_min;     /* dense trailing blocks at least this wide update
+                                  on the tensor cores (tcgen05, FP32 accuracy by
+                                  a three-term TF32 split); 0: FP32 FMA always  */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

@@ -1,0 +1,111 @@
+"""The tensor-core trailing update of the dense tail (tcgen05, 3xTF32) against
+the oracle's FP32 column algorithm.
+
+The tensor-core path is forced on small trailing blocks (dense_tc_min low) so
+that partial 128 x 128 tiles, a short last panel, the panel pairs of the
+look-ahead (forced with dense_lookahead) and both tail layouts (in place in the
+CSC values, and the gathered buffer of the mesh) are exercised; each must stay
+within the factor tolerance (per-column max-relative difference <= 1e-4) and
+the profile must show the tensor-core kernel, not the FP32 FMA one, ran.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+from test_gpu_parity import FACTOR_TOL, col_max_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _factor(A, perturb=False, **tune):
+    import pyglu
+    from pyglu import _capi, autotune
+
+    lu = pyglu.GLUFactorization(*A, perturb=perturb)
+    autotune._set(lu.handle, tune)
+    eng = _capi.engine()
+    _capi.check(eng.glu_profile_enable(lu.handle, 1))
+    lu.refactor(A[0])
+    kt = _capi.kernel_times(lu.handle)
+    _capi.check(eng.glu_profile_enable(lu.handle, 0))
+    return lu, kt
+
+
+def _check(lu, perturb=False):
+    p = lu.pattern()
+    lp, li = lu.levels()
+    v0 = lu.analysis.predict_lu()
+    pert = oracle.pert(p, v0) if perturb else 0.0
+    ref = oracle.factor(p, v0, lp, li, np.float32, pert)
+    v = lu.lu_values()
+    assert np.isfinite(v).all()
+    return col_max_rel(v, ref, p["sym_c_ptr"])
+
+
+CASES = {
+    # name: (generator, tuning)
+    "nodal1500_tc": (lambda s: s.nodal(1500, seed=2), {"dense_tc_min": 128}),
+    "nodal2500_tc_pairs": (lambda s: s.nodal(2500, seed=9), {"dense_tc_min": 128, "dense_lookahead": 256}),
+    "config0_tc_pairs": (lambda s: s.config0(), {"dense_tc_min": 128, "dense_lookahead": 512}),
+    "mesh90_buffer_tc": (lambda s: s.grid_mesh(side=90, seed=3, n_long=40), {"dense_tc_min": 64}),
+    "nodal_band32_tc_pairs": (lambda s: s.nodal(3000, seed=12, band=32, n_long=2, unsym_frac=0.1),
+                              {"dense_tc_min": 128, "dense_lookahead": 256}),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tensor_core_update_matches_oracle(name):
+    from pyglu import synth
+
+    gen, tune = CASES[name]
+    A = gen(synth)
+    lu, kt = _factor(A, **tune)
+    m = lu.stats["dense_tail"]
+    assert m >= tune["dense_tc_min"], m
+    assert kt["k_dense_update_tc"][1] > 0 and kt["k_dense_pack"][1] > 0, kt
+    assert kt["k_dense_update"][1] == 0, kt
+    err = _check(lu)
+    assert err <= FACTOR_TOL, err
+
+
+def test_tensor_core_update_with_gesp():
+    from pyglu import synth
+
+    A = synth.nodal(2000, seed=4)
+    lu, kt = _factor(A, perturb=True, dense_tc_min=128, dense_lookahead=256)
+    assert kt["k_dense_update_tc"][1] > 0
+    err = _check(lu, perturb=True)
+    assert err <= FACTOR_TOL, err
+
+
+def test_tensor_core_batch_of_value_sets():
+    """Several value sets in one launch sequence (blockIdx.z of the packs and
+    the tile index of the persistent update): every set against the oracle."""
+    import pyglu
+    from pyglu import _capi, autotune, synth
+
+    A = synth.nodal(2000, seed=12, band=32, n_long=2, unsym_frac=0.1)
+    vals = synth.perturb_values(*A, count=3, seed=1)
+    bl = pyglu.BatchedGLU(A[1], A[2], A[3], vals)
+    autotune._set(bl.handle, {"dense_tc_min": 128, "dense_lookahead": 256})
+    bl.refactor(vals)
+    an = bl._an
+    p = an.pattern()
+    lp, li = oracle.leveling(p)
+    for z in range(3):
+        placed = np.zeros(an.nnz_lu, np.float32)
+        placed[an.src_slot] = (vals[z] * an.src_scale).astype(np.float32)
+        ref = oracle.factor(p, placed, lp, li, np.float32)
+        v = np.empty(an.nnz_lu, np.float32)
+        _capi.check(_capi.engine().glu_store_lu_values(bl.handle, z, 1, _capi.ptr(v), _capi.GLU_HOST, None))
+        assert col_max_rel(v, ref, p["sym_c_ptr"]) <= FACTOR_TOL, z
+
+
+def test_fma_path_still_selectable():
+    from pyglu import synth
+
+    A = synth.nodal(2500, seed=9)
+    lu, kt = _factor(A, dense_tc_min=0)
+    assert kt["k_dense_update_tc"][1] == 0 and kt["k_dense_update"][1] > 0
+    assert _check(lu) <= FACTOR_TOL
