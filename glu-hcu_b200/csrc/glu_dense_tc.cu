@@ -8,10 +8,9 @@
 //     a b ~= a_lo b_hi + a_hi b_lo + a_hi b_hi,
 // accumulated in FP32 in tensor memory.  The dropped a_lo b_lo term and the
 // rounding of a_lo are below 2^-21 relative to |a b|, so each product carries
-// close to FP32 accuracy; the entry is then updated once, c - sum_k l_ik u_kj,
-// instead of once per k as in the FP32 FMA kernel (same bound on the error of
-// a sum of K products; the entries still receive each panel's contribution
-// in panel order).
+// close to FP32 accuracy.  An entry receives one partial sum per 32-wide K
+// chunk, c := c - sum_{k in chunk} l_ik u_kj, in K order, instead of one
+// update per k as in the FP32 FMA kernel.
 //
 // Data flow per update:
 //   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
@@ -23,10 +22,15 @@
 //        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 32 FP32
 //                 operand boxes (128-byte swizzle) into a 3-stage ring;
 //        warp 1   MMA issuer: 3 x 4 tcgen05.mma (M = N = 128, K = 8, kind
-//                 tf32) per stage into one of two TMEM accumulators;
+//                 tf32) per stage into one of two TMEM accumulators, which
+//                 then holds that K chunk's partial sum;
 //        warps 2-5 epilogue: load the C tile from HBM into registers while
-//                 the MMAs run, then tcgen05.ld the accumulator, subtract,
-//                 store; the other accumulator takes the next tile's MMAs.
+//                 the MMAs run, tcgen05.ld each chunk's partial sum and
+//                 subtract it (FP32, round to nearest), store the tile; the
+//                 other accumulator takes the next chunk's MMAs.
+//      The tensor core's FP32 accumulation truncates; handing every 32-wide K
+//      chunk (12 MMAs) to the epilogue keeps that error to a few units in the
+//      last place of the chunk's sum, comparable to the FMA path's rounding.
 //      C stays where it lies (element (i, j) at val[doff[j] + i]), so in-place
 //      tails with irregular column offsets need no copy.
 // All waits on mbarriers are bounded (spin_limit polls); a wait that runs out
@@ -305,23 +309,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp == 1) {
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
-            uint32_t g = 0, i = 0;
+            uint32_t g = 0;  // stages consumed
+            uint32_t u = 0;  // accumulator rounds: one per (tile, K chunk)
             bool ok = true;
-            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x, ++i) {
-                const uint32_t a = i & 1, aph = (i >> 1) & 1;
-                if (!mbar_wait(&acc_empty[a], aph ^ 1, spin_limit)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t d = tmem + a * kTile;
-                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g) {
+            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g, ++u) {
+                    const uint32_t a = u & 1, aph = (u >> 1) & 1;
                     const uint32_t s = g % kStages, ph = (g / kStages) & 1;
-                    if (!mbar_wait(&full[s], ph, spin_limit)) {
+                    if (!mbar_wait(&acc_empty[a], aph ^ 1, spin_limit) || !mbar_wait(&full[s], ph, spin_limit)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
+                    const uint32_t d = tmem + a * kTile;
                     const uint32_t base = smem_addr(smem + s * kStageBytes);
 #pragma unroll
                     for (uint32_t k8 = 0; k8 < kChunk / 8; ++k8) {
@@ -330,14 +330,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const uint64_t al = kmajor_sw128_desc(base + kOpBytes + off);
                         const uint64_t bh = kmajor_sw128_desc(base + 2 * kOpBytes + off);
                         const uint64_t bl = kmajor_sw128_desc(base + 3 * kOpBytes + off);
-                        tc_mma_tf32(d, al, bh, (kc | k8) != 0);
+                        tc_mma_tf32(d, al, bh, k8 != 0);
                         tc_mma_tf32(d, ah, bl, 1);
                         tc_mma_tf32(d, ah, bh, 1);
                     }
                     tc_commit(&empty[s]);
+                    tc_commit(&acc_full[a]);
                 }
-                if (!ok) break;
-                tc_commit(&acc_full[a]);
             }
             if (!ok) atomicOr(status, DEV_TIMEOUT);
             tc_commit(done);
@@ -360,10 +359,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
         }
-        uint32_t i = 0;
-        for (uint32_t t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+        uint32_t u = 0;  // accumulator rounds, as the MMA issuer counts them
+        for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
             const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
-            const uint32_t a = i & 1, aph = (i >> 1) & 1;
             float *val = val_base + tl.z * stride;
             const bool rok = tl.rbase + row < reg.r_hi;
             const uint32_t grow = r0 + tl.rbase + row;
@@ -384,26 +382,39 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
                     c[cc][jj] = ok ? ld_cg(val + o + grow) : 0.0f;
                 }
-            // warp-uniform: the tcgen05.ld below needs the whole warp
-            if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[a], aph, spin_limit))) {
+            // the chunks' partial sums, subtracted in K order in FP32
+            bool ok = true;
+            for (uint32_t kc = 0; kc < nchunks; ++kc, ++u) {
+                const uint32_t a = u & 1, aph = (u >> 1) & 1;
+                // warp-uniform: the tcgen05.ld below needs the whole warp
+                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[a], aph, spin_limit))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int cc = 0; cc < 4; ++cc) {
+                    float acc[32];
+                    tc_ld32(tmem + ((q * 32) << 16) + a * kTile + cc * 32, acc);
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[a]);
+            }
+            if (!ok) {
                 if (lane == 0) atomicOr(status, DEV_TIMEOUT);
                 break;
             }
-            tc_fence_after();
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                float acc[32];
-                tc_ld32(tmem + ((q * 32) << 16) + a * kTile + cc * 32, acc);
+            for (int cc = 0; cc < 4; ++cc)
 #pragma unroll
                 for (int jj = 0; jj < 32; ++jj) {
                     const uint32_t o = __shfl_sync(0xffffffffu, coff[cc], jj);
-                    const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
-                    if (ok) st_cg(val + o + grow, c[cc][jj] - acc[jj]);
+                    const bool okc = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
+                    if (okc) st_cg(val + o + grow, c[cc][jj]);
                 }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[a]);
         }
     }
     __syncthreads();

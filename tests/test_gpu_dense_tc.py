@@ -66,6 +66,7 @@ def test_tensor_core_update_matches_oracle(name):
     assert kt["k_dense_update_tc"][1] > 0 and kt["k_dense_pack"][1] > 0, kt
     assert kt["k_dense_update"][1] == 0, kt
     err = _check(lu)
+    print(f"{name}: m={m} max column relative difference {err:.3e}")
     assert err <= FACTOR_TOL, err
 
 
