@@ -283,7 +283,7 @@ void find_full_tail(const SymbolicData &s, uint32_t min_m, uint32_t &t, uint32_t
 // the columns < t at kSparseRate plus kLevelLatency per level that still has
 // an active column < t.  Returns the t of least estimated time with
 // m <= max_m (t = n: no dense tail).
-constexpr double kDenseRate = 30e12, kPanelLatency = 20e-6;
+constexpr double kDenseRate = 30e12, kDenseRateTc = 120e12, kPanelLatency = 20e-6;
 // Default width from which trailing blocks factor with panel look-ahead.
 constexpr uint32_t kLookaheadMin = 3072;
 // Default width from which trailing blocks update on the tensor cores.
@@ -291,7 +291,7 @@ constexpr uint32_t kDenseTcMin = 1024;
 constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
 
 uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
-                      const std::vector<int32_t> &level_idx, uint32_t max_m) {
+                      const std::vector<int32_t> &level_idx, uint32_t max_m, const glu_tuning &tu) {
     const uint32_t n = s.n;
     // sparse work of column k and the first column of each level
     std::vector<double> pre(n + 1, 0.0);
@@ -319,7 +319,9 @@ uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_p
     for (int64_t tt = n; tt >= lo; tt -= 16) {
         const uint32_t t = uint32_t(tt);
         double m = double(n - t);
-        double dense = m > 0 ? (2.0 / 3.0) * m * m * m / kDenseRate + std::ceil(m / kDenseNB) * kPanelLatency : 0;
+        const double rate = tu.dense_rate ? 1e9 * tu.dense_rate
+                                          : (tu.dense_tc_min && m >= tu.dense_tc_min ? kDenseRateTc : kDenseRate);
+        double dense = m > 0 ? (2.0 / 3.0) * m * m * m / rate + std::ceil(m / kDenseNB) * kPanelLatency : 0;
         double nlev = double(std::lower_bound(lev_first.begin(), lev_first.end(), t) - lev_first.begin());
         double sparse = pre[t] / kSparseRate + nlev * kLevelLatency;
         if (dense + sparse < best) {
@@ -660,7 +662,7 @@ Status build_plan(glu_handle_s *h) {
             if (cap < max_m) max_m = uint32_t(cap);
         }
     }
-    uint32_t t_opt = choose_split(s, h->level_ptr, h->level_idx, std::max(max_m, m_full));
+    uint32_t t_opt = choose_split(s, h->level_ptr, h->level_idx, std::max(max_m, m_full), h->tune);
     h->dense_buffer = false;
     if (t_opt >= t_full) {
         h->t = t_opt;  // any trailing block of a fully dense block is fully dense
@@ -842,7 +844,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");

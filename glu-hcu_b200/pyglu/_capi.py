@@ -79,7 +79,8 @@ class Tuning(C.Structure):
     _fields_ = [("wide_work", C.c_uint32), ("chain_cluster", C.c_uint32), ("group_lanes", C.c_uint32),
                 ("dense_tail_min", C.c_uint32), ("dense_tail_max", C.c_uint32), ("solve_thin", C.c_uint32),
                 ("solve_cluster", C.c_uint32), ("sn_width", C.c_uint32),
-                ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32), ("dense_tc_min", C.c_uint32)]
+                ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32), ("dense_tc_min", C.c_uint32),
+                ("dense_rate", C.c_uint32)]
 
 
 _vp = C.c_void_p

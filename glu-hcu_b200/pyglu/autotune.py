@@ -1,14 +1,29 @@
 """Schedule autotuner.
 
-Searches the engine's schedule knobs (glu_tuning: work threshold that sends a
-level to its own launch, cluster size of the narrow-level kernel, lanes per
-update item, smallest dense trailing block) by timing real factorizations on
-the device, and caches the winner per (pattern hash, GPU name) in a JSON file.
+The reference fixes its schedule in code: a level's columns go to blocks of
+2, 4 or 32 warps by level size (896 / 448 / 16 thresholds) and narrow levels
+spread over 16 streams (src/numeric.cu:390, 557-565).  Here the engine's
+schedule knobs (glu_tuning) are chosen per pattern by timing real
+factorizations on the device, and the winner is cached per (pattern, GPU,
+batch) in a JSON file.
+
+Search: coordinate descent from the engine's defaults over the knobs the
+factorization path in use reads --
+
+* supernodal path (sn_width > 0, the default): widest supernode, grouping of
+  small supernodes into warps, the split between sparse part and dense
+  trailing block (the cost model's dense rate and the largest buffered
+  block), the width from which the dense block takes its panels in
+  look-ahead pairs, the width from which it updates on the tensor cores;
+* column path (sn_width = 0): lanes per update, the cluster size of the
+  narrow-level kernel, the work that sends a level to its own launch.
+
+Each knob takes its values in turn with the others held; the fastest
+refactorization (median of ``repeats``) is kept; two passes.
 """
 from __future__ import annotations
 
 import hashlib
-import itertools
 import json
 import os
 
@@ -17,6 +32,21 @@ import numpy as np
 from . import _capi
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "glu_b200", "tune.json")
+
+# values tried per knob (the engine's default is always tried first)
+SUPERNODAL_SPACE = {
+    "sn_width": [16, 32, 64],
+    "sn_small": [0, 1],
+    "dense_rate": [0, 15_000, 60_000, 250_000],
+    "dense_tail_max": [2048, 4096, 8192],
+    "dense_lookahead": [0, 1024, 3072],
+    "dense_tc_min": [0, 512, 1024, 2048],
+}
+COLUMN_SPACE = {
+    "group_lanes": [0, 8, 32],
+    "chain_cluster": [8, 16],
+    "wide_work": [50_000, 200_000, 1_000_000],
+}
 
 
 def _pattern_key(an):
@@ -48,55 +78,79 @@ def _set(handle, cfg):
     _capi.check(_capi.engine().glu_set_tuning(handle, _capi.C.byref(t)), "set tuning")
 
 
-def candidates():
-    """The search space (small grid)."""
-    grid = dict(wide_work=[50_000, 200_000, 1_000_000], chain_cluster=[8, 16], group_lanes=[0, 8, 32])
-    keys = list(grid)
-    for vals in itertools.product(*(grid[k] for k in keys)):
-        yield dict(zip(keys, vals))
+def current(handle):
+    """The handle's schedule knobs as a dict."""
+    t = _get(handle)
+    return {k: getattr(t, k) for k, _ in _capi.Tuning._fields_}
 
 
-def tune(lu, data=None, repeats=3, cache=DEFAULT_CACHE, space=None, use_cache=True):
+def _time(lu, values, repeats):
+    times = []
+    for _ in range(repeats):
+        lu.refactor(values)
+        times.append(lu.stats["last_factor_ms"])
+    return float(np.median(times))
+
+
+def _space_for(cfg, space):
+    if space is not None:
+        return space
+    return SUPERNODAL_SPACE if cfg.get("sn_width", 1) else COLUMN_SPACE
+
+
+def tune(lu, data=None, repeats=3, cache=DEFAULT_CACHE, space=None, use_cache=True, passes=2):
     """Pick the fastest schedule for ``lu`` (a GLUFactorization or BatchedGLU).
 
     ``data`` are the values to factor while timing (default: the analysed
-    ones).  Returns (best_config, best_ms).  The handle keeps the winner.
+    ones; for a batch, its value array).  ``space`` overrides the knob grid
+    (a dict knob -> list of values).  Returns (best_config, best_ms,
+    report) where report holds the default's time and every trial; the handle
+    keeps the winner and is left factored with ``data``.
     """
     an = lu._an
     h = lu.handle
-    key = f"{_pattern_key(an)}:{_gpu_name()}:{getattr(lu, 'batch', 1)}"
+    batch = getattr(lu, "batch", 1)
+    values = (an.data if data is None else data) if batch == 1 else data
+    if values is None:
+        raise ValueError("a batch needs its value sets to time")
+    key = f"{_pattern_key(an)}:{_gpu_name()}:{batch}"
     if use_cache and cache and os.path.exists(cache):
         try:
             with open(cache) as f:
                 db = json.load(f)
             if key in db:
                 _set(h, db[key]["config"])
-                lu.refactor(an.data if data is None else data) if getattr(lu, "batch", 1) == 1 else None
-                return db[key]["config"], db[key]["ms"]
+                lu.refactor(values)
+                return db[key]["config"], db[key]["ms"], {"cached": True}
         except (OSError, ValueError):
             pass
-    values = an.data if data is None else data
-    best, best_ms = None, float("inf")
-    for cfg in (space if space is not None else candidates()):
-        try:
-            _set(h, cfg)
-        except ValueError:
-            continue
-        times = []
-        for _ in range(repeats):
-            if getattr(lu, "batch", 1) == 1:
-                lu.refactor(values)
-            else:
-                lu.refactor(values)
-            times.append(lu.stats["last_factor_ms"])
-        ms = float(np.median(times))
-        if ms < best_ms:
-            best, best_ms = cfg, ms
+    base = current(h)
+    best = dict(base)
+    best_ms = _time(lu, values, repeats)
+    report = {"default_ms": best_ms, "trials": [], "cached": False}
+    grid = _space_for(base, space)
+    for _ in range(passes):
+        improved = False
+        for knob, choices in grid.items():
+            for v in choices:
+                if v == best.get(knob):
+                    continue
+                cfg = dict(best)
+                cfg[knob] = v
+                try:
+                    _set(h, cfg)
+                except (ValueError, _capi.GLUError):
+                    continue
+                ms = _time(lu, values, repeats)
+                report["trials"].append((knob, v, ms))
+                if ms < best_ms:
+                    best, best_ms, improved = cfg, ms, True
+        if not improved:
+            break
     _set(h, best)
-    if getattr(lu, "batch", 1) == 1:
-        lu.refactor(values)
-    else:
-        lu.refactor(values)
+    lu.refactor(values)
+    changed = {k: v for k, v in best.items() if base.get(k) != v}
+    report["changed"] = changed
     if cache:
         try:
             os.makedirs(os.path.dirname(cache), exist_ok=True)
@@ -109,4 +163,4 @@ def tune(lu, data=None, repeats=3, cache=DEFAULT_CACHE, space=None, use_cache=Tr
                 json.dump(db, f, indent=1)
         except (OSError, ValueError):
             pass
-    return best, best_ms
+    return best, best_ms, report

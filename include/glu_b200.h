@@ -248,6 +248,9 @@ typedef struct {
     uint32_t dense_tc_min;     /* dense trailing blocks at least this wide update
                                   on the tensor cores (tcgen05, FP32 accuracy by
                                   a three-term TF32 split); 0: FP32 FMA always  */
+    uint32_t dense_rate;       /* dense-block throughput (GFLOP/s) the split cost
+                                  model assumes; 0: built in (FMA or tensor-core
+                                  rate, whichever the block would use)           */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);
