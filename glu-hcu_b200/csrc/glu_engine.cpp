@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -44,6 +45,16 @@ static Status cuda_fail(cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_fail(e_, (what));  \
     } while (0)
 
+// Device allocations still to fail (GLU_INJECT_ALLOC_FAILURES).
+static std::atomic<int> g_fail_allocs{0};
+
+static bool injected_alloc_failure() {
+    int v = g_fail_allocs.load(std::memory_order_relaxed);
+    while (v > 0)
+        if (g_fail_allocs.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return true;
+    return false;
+}
+
 // Device buffer owned by a handle.
 struct DevBuf {
     void *p = nullptr;
@@ -57,6 +68,7 @@ struct DevBuf {
     cudaError_t alloc(size_t b) {
         release();
         if (b == 0) return cudaSuccess;
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMalloc(&p, b);
         if (e == cudaSuccess) bytes = b;
         return e;
@@ -213,6 +225,7 @@ struct glu_handle_s {
     uint32_t pack_m = 0;
     uint32_t num_sms = 148;
     uint32_t spin_limit = kSpinLimit;
+    bool inject_unset_flag = false;  // GLU_INJECT_UNSET_SOLVE_FLAG, for the next solve
     KernelProfiler prof;
     bool factored = false;
     glu_stats stats{};
@@ -770,6 +783,8 @@ Status build_plan(glu_handle_s *h) {
     h->S.doff = h->d_doff.as<uint32_t>();
     h->S.tail_start = h->d_tail_start.as<uint32_t>();
     h->S.cluster = h->tune.solve_cluster ? h->tune.solve_cluster : 4;
+    h->S.spin_limit = h->spin_limit;
+    h->S.ticket_base = 0;
     {
         // CSR position of the first column >= t in every tail row
         std::vector<uint32_t> trs(std::max<uint32_t>(m, 1), 0);
@@ -949,6 +964,17 @@ Status read_status(glu_handle_s *h, cudaStream_t st, uint32_t *flags) {
     return GLU_OK;
 }
 
+// The solve plan of the next solve: the handle's, with a pending
+// GLU_INJECT_UNSET_SOLVE_FLAG applied (and consumed).
+SolvePlanDev solve_plan(glu_handle_s *h) {
+    SolvePlanDev S = h->S;
+    if (h->inject_unset_flag) {
+        S.ticket_base = 1;
+        h->inject_unset_flag = false;
+    }
+    return S;
+}
+
 // One FP32 solve of y in place (nrhs vectors of n), in the permuted system,
 // with the factors of value set z.
 Status solve_inplace(glu_handle_s *h, uint32_t z, float *y, uint32_t nrhs, bool trans, cudaStream_t st) {
@@ -959,12 +985,13 @@ Status solve_inplace(glu_handle_s *h, uint32_t z, float *y, uint32_t nrhs, bool 
     const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(z) * h->m * h->m : val;
     GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs), "allocate solve buffer");
     float *xo = h->d_xo.as<float>();
+    const SolvePlanDev S = solve_plan(h);
     if (!trans) {
-        GLU_CUDA(solve_lower_unit(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "lower solve");
-        GLU_CUDA(solve_upper(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "upper solve");
+        GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "lower solve");
+        GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "upper solve");
     } else {
-        GLU_CUDA(solve_upper_trans(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st), "transposed upper solve");
-        GLU_CUDA(solve_lower_unit_trans(h->P, h->S, val, dval, y, xo, nrhs, cnt, tk, status, st),
+        GLU_CUDA(solve_upper_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "transposed upper solve");
+        GLU_CUDA(solve_lower_unit_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st),
                  "transposed lower solve");
     }
     return GLU_OK;
@@ -1031,8 +1058,9 @@ Status solve_f32_scratch(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const fl
     const float *val = h->d_val.as<float>() + size_t(inst) * h->nnz;
     const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(inst) * h->m * h->m : val;
     uint32_t *status = h->d_status.as<uint32_t>();
-    GLU_CUDA(solve_lower_unit(h->P, h->S, val, dval, y, xo, nrhs, flags, ticket, status, st), "lower solve");
-    GLU_CUDA(solve_upper(h->P, h->S, val, dval, y, xo, nrhs, flags, ticket, status, st), "upper solve");
+    const SolvePlanDev S = solve_plan(h);
+    GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, st), "lower solve");
+    GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, st), "upper solve");
     GLU_CUDA(launch_transform_f32(T.out_idx, T.out_scale, y, x, h->n, nrhs, st), "transform");
     uint32_t fl = 0;
     Status s = read_status(h, st, &fl);
@@ -1651,6 +1679,28 @@ glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches) {
 
 const char *glu_kernel_kind_name(int kind) {
     return (kind >= 0 && kind < GLU_KERNEL_KINDS) ? kKindNames[kind] : "";
+}
+
+glu_status glu_set_wait_limit(glu_handle_t h, uint32_t polls) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    h->spin_limit = polls ? polls : kSpinLimit;
+    h->S.spin_limit = h->spin_limit;
+    return GLU_OK;
+}
+
+glu_status glu_debug_inject(glu_handle_t h, int what, uint32_t value) {
+    switch (what) {
+        case GLU_INJECT_ALLOC_FAILURES:
+            g_fail_allocs.store(int(std::min<uint32_t>(value, 1u << 30)), std::memory_order_relaxed);
+            return GLU_OK;
+        case GLU_INJECT_UNSET_SOLVE_FLAG:
+            if (!h) return set_error(GLU_ERR_ARG, "null handle");
+            if (h->m == 0) return set_error(GLU_ERR_UNSUPPORTED, "the factorization has no dense trailing block");
+            h->inject_unset_flag = true;
+            return GLU_OK;
+        default:
+            return set_error(GLU_ERR_ARG, "unknown injection %d", what);
+    }
 }
 
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t) {

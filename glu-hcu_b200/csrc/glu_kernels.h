@@ -193,6 +193,9 @@ struct SolvePlanDev {
     SweepPlan sweep[4];             // L, U, U^T, L^T
     SnSweepPlan sn[2];              // supernodal L and U sweeps (nlev == 0: column sweeps)
     uint32_t cluster;               // CTAs of the thin-level cluster kernel
+    uint32_t spin_limit;            // polls of a device-side wait before it gives up
+    uint32_t ticket_base;           // first block ticket of the dense sweeps (0; 1 leaves the first
+                                    // block's flag unset: a diagnostic of the bounded waits)
 };
 
 // Supernodal sweep over the columns [0, t) (forward L, or backward U), then

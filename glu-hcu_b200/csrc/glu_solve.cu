@@ -27,11 +27,13 @@ namespace cg = cooperative_groups;
 
 namespace glu {
 
-// Bounded wait until *cnt reaches target.  Returns false on timeout.
-__device__ __forceinline__ bool wait_count(const uint32_t *cnt, uint32_t target, uint32_t *status) {
+// Bounded wait until *cnt reaches target (at most `limit` polls).  Returns
+// false on timeout.
+__device__ __forceinline__ bool wait_count(const uint32_t *cnt, uint32_t target, uint32_t *status,
+                                           uint32_t limit) {
     uint32_t spins = 0;
     while (ld_acquire_gpu(cnt) < target) {
-        if (++spins > kSpinLimit) {
+        if (++spins > limit) {
             atomicOr(status, DEV_TIMEOUT);
             return false;
         }
@@ -210,7 +212,8 @@ constexpr int kRHSChunk = 4;
 template <int kMode>
 __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ val, const uint32_t *__restrict__ doff,
                                                     uint32_t t, uint32_t m, float *y, uint32_t n, uint32_t nrhs,
-                                                    uint32_t *flags, uint32_t *ticket, uint32_t *status) {
+                                                    uint32_t *flags, uint32_t *ticket, uint32_t *status,
+                                                    uint32_t spin_limit, uint32_t ticket_base) {
     constexpr bool kLower = (kMode == 0 || kMode == 2);
     constexpr bool kTrans = (kMode >= 2);
     constexpr bool kUnit = (kMode == 0 || kMode == 3);
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     __shared__ uint32_t s_blk;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = (m + kRB - 1) / kRB;
-    if (tid == 0) s_blk = atomicAdd(ticket, 1u);
+    if (tid == 0) s_blk = atomicAdd(ticket, 1u) + ticket_base;
     __syncthreads();
     const uint32_t tk = s_blk;
     if (tk >= nb) return;
@@ -264,7 +267,7 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
                     tile[i][cc] = tv[qq];
                 }
             }
-            if (tid == 0) wait_count(flags + c, 1u, status);
+            if (tid == 0) wait_count(flags + c, 1u, status, spin_limit);
             __syncthreads();
             for (uint32_t e = tid; e < kRB * kRHSChunk; e += 256) {
                 uint32_t cc = e / kRHSChunk, r = e % kRHSChunk;
@@ -339,7 +342,8 @@ static cudaError_t dense_sweep(const SolvePlanDev &S, const float *dval, float *
     cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * nb, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    k_dense_trsv<kMode><<<nb, 256, 0, st>>>(dval, S.doff, S.t, S.m, y, n, nrhs, flags, ticket, status);
+    k_dense_trsv<kMode><<<nb, 256, 0, st>>>(dval, S.doff, S.t, S.m, y, n, nrhs, flags, ticket, status,
+                                            S.spin_limit, S.ticket_base);
     return cudaGetLastError();
 }
 

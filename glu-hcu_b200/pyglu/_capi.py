@@ -27,6 +27,8 @@ GLU_ERR_NO_DEVICE = -8
 GLU_ERR_UNSUPPORTED = -9
 GLU_HOST = 0
 GLU_DEVICE = 1
+GLU_INJECT_ALLOC_FAILURES = 1
+GLU_INJECT_UNSET_SOLVE_FLAG = 2
 
 # Every symbol the engine exports (checked by the tests against the header).
 ENGINE_SYMBOLS = [
@@ -36,7 +38,7 @@ ENGINE_SYMBOLS = [
     "glu_set_source", "glu_load_lu_values", "glu_store_lu_values", "glu_load_source_values",
     "glu_factor", "glu_solve", "glu_solve_transposed", "glu_solve_refined", "glu_get_stats",
     "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
-    "glu_kernel_kind_name", "glu_measure_fp32_peak",
+    "glu_kernel_kind_name", "glu_measure_fp32_peak", "glu_set_wait_limit", "glu_debug_inject",
 ]
 GLU_KERNEL_KINDS = 14
 PRE_SYMBOLS = [
@@ -124,6 +126,8 @@ def load_engine():
         "glu_profile_enable": [_vp, C.c_int],
         "glu_kernel_times": [_vp, _vp, _vp],
         "glu_measure_fp32_peak": [C.c_int, C.POINTER(C.c_double)],
+        "glu_set_wait_limit": [_vp, _u32],
+        "glu_debug_inject": [_vp, C.c_int, _u32],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -228,6 +228,27 @@ const char *glu_kernel_kind_name(int kind);
  * roofline.  No counterpart in the reference. */
 glu_status glu_measure_fp32_peak(int device, double *tflops);
 
+/* Device-side waits of the handle's kernels (the dense-tail solve's block
+ * flags, the tensor-core update's pipeline barriers) give up after `polls`
+ * polls: the kernel sets a status flag, finishes without further waiting, and
+ * the call returns GLU_ERR_TIMEOUT with the handle still usable.  0 restores
+ * the default (2^24 polls, a few seconds).  The reference has no bounded
+ * waits: a stuck kernel blocks its per-level cudaDeviceSynchronize
+ * (src/numeric.cu:615-616) forever. */
+glu_status glu_set_wait_limit(glu_handle_t h, uint32_t polls);
+
+/* Failure injection for tests of the error paths; no counterpart in the
+ * reference.  Nothing here faults or hangs a GPU: the failures are made on
+ * the host or are a flag that nothing sets, met by a bounded wait.
+ *   GLU_INJECT_ALLOC_FAILURES: the next `value` device allocations of the
+ *     library fail as out of memory (process-wide; h may be NULL).
+ *   GLU_INJECT_UNSET_SOLVE_FLAG: in the next solve of h, the dense-tail
+ *     sweeps start their block tickets at 1, so no block sets the first
+ *     block's completion flag and every block that needs it waits until the
+ *     wait limit; the call returns GLU_ERR_TIMEOUT (value ignored). */
+typedef enum { GLU_INJECT_ALLOC_FAILURES = 1, GLU_INJECT_UNSET_SOLVE_FLAG = 2 } glu_inject;
+glu_status glu_debug_inject(glu_handle_t h, int what, uint32_t value);
+
 /* Schedule knobs (the autotuner's search space).  Applies to later calls. */
 typedef struct {
     uint32_t wide_work;        /* a level with more update work runs alone       */

@@ -138,3 +138,12 @@ def test_oracle_unaffected_by_checks(pattern):
     lp, li = oracle.leveling(pattern)
     assert lp[-1] == pattern["sym_c_ptr"].size - 1
     assert np.array_equal(np.sort(li), np.arange(li.size))
+
+
+def test_failure_injection_arguments():
+    eng = _capi.engine()
+    assert eng.glu_debug_inject(None, 99, 0) == _capi.GLU_ERR_ARG
+    assert eng.glu_debug_inject(None, _capi.GLU_INJECT_UNSET_SOLVE_FLAG, 0) == _capi.GLU_ERR_ARG
+    assert eng.glu_set_wait_limit(None, 10) == _capi.GLU_ERR_ARG
+    assert eng.glu_debug_inject(None, _capi.GLU_INJECT_ALLOC_FAILURES, 3) == _capi.GLU_OK
+    assert eng.glu_debug_inject(None, _capi.GLU_INJECT_ALLOC_FAILURES, 0) == _capi.GLU_OK
