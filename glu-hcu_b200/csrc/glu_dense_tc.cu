@@ -2,35 +2,37 @@
 //
 // The blocked dense LU of the trailing block (glu_factor_dense.cu) spends
 // almost all of its flops in A22 -= L21 U12 with K = 64 or 128 (one panel or a
-// pair).  Here that product runs as tcgen05.mma with FP32 accuracy kept by the
-// three-term TF32 split ("3xTF32"): with a = a_hi + a_lo, a_hi = rna_tf32(a),
-// a_lo = rna_tf32(a - a_hi) (and the same for b),
-//     a b ~= a_lo b_hi + a_hi b_lo + a_hi b_hi,
-// accumulated in FP32 in tensor memory.  The dropped a_lo b_lo term and the
-// rounding of a_lo are below 2^-21 relative to |a b|, so each product carries
-// close to FP32 accuracy.  An entry receives one partial sum per 32-wide K
-// chunk, c := c - sum_{k in chunk} l_ik u_kj, in K order, instead of one
-// update per k as in the FP32 FMA kernel.
-//
+// pair).  Here that product runs as tcgen05.mma kind::tf32 with FP32 accuracy
+// kept by splitting every operand into three TF32 parts,
+//     a = a0 + a1 + a2,  a0 = rna_tf32(a), a1 = rna_tf32(a - a0),
+//                        a2 = rna_tf32(a - a0 - a1)
+// (exact: 3 x 11 significant bits cover FP32's 24), and keeping every
+// product term down to 2^-22 relative:
+//     a b ~= a0 b0 + (a0 b1 + a1 b0) + (a0 b2 + a1 b1 + a2 b0),
+// whose error, below 2^-32 |a b|, is far under FP32 rounding.  The big term
+// a0 b0 (exact in FP32) and the small terms go to separate FP32 accumulators
+// in tensor memory, so the tensor core's truncating accumulation of the big
+// term runs over four MMAs per 32-wide K chunk and that of the small terms
+// stays 2^-11 below it.  Each chunk's two partial sums are then subtracted from
+// the entry in FP32 with round to nearest, c := (c - big) - small, in K order.
+
 // Data flow per update:
 //   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
-//      split into TF32 hi/lo parts, written K-major as rows of 256 floats
-//      (slots 0..127 hi, 128..255 lo; the first panel of a pair fills slots
-//      0..63, the second 64..127) -- the operand layout the MMA reads.
+//      split into their three TF32 parts, written K-major as rows of 384
+//      floats (slots 0..127 part 0, 128..255 part 1, 256..383 part 2; the
+//      first panel of a pair fills slots 0..63 of each part, the second
+//      64..127) -- the operand layout the MMA reads.
 //   2. k_dense_update_tc, persistent (one CTA per SM), per 128 x 128 tile of
 //      the trailing block:
 //        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 32 FP32
-//                 operand boxes (128-byte swizzle) into a 3-stage ring;
-//        warp 1   MMA issuer: 3 x 4 tcgen05.mma (M = N = 128, K = 8, kind
-//                 tf32) per stage into one of two TMEM accumulators, which
-//                 then holds that K chunk's partial sum;
+//                 operand boxes (128-byte swizzle), three parts of A and of B
+//                 per 32-wide K chunk, into a 2-stage ring;
+//        warp 1   MMA issuer: 6 x 4 tcgen05.mma (M = N = 128, K = 8) per
+//                 chunk into one of two accumulator pairs (big, small);
 //        warps 2-5 epilogue: load the C tile from HBM into registers while
-//                 the MMAs run, tcgen05.ld each chunk's partial sum and
-//                 subtract it (FP32, round to nearest), store the tile; the
-//                 other accumulator takes the next chunk's MMAs.
-//      The tensor core's FP32 accumulation truncates; handing every 32-wide K
-//      chunk (12 MMAs) to the epilogue keeps that error to a few units in the
-//      last place of the chunk's sum, comparable to the FMA path's rounding.
+//                 the MMAs run, tcgen05.ld each chunk's two partial sums and
+//                 subtract them, store the tile; the other accumulator pair
+//                 takes the next chunk's MMAs.
 //      C stays where it lies (element (i, j) at val[doff[j] + i]), so in-place
 //      tails with irregular column offsets need no copy.
 // All waits on mbarriers are bounded (spin_limit polls); a wait that runs out
@@ -52,11 +54,13 @@ namespace {
 
 constexpr int kTile = 128;                               // M = N of an update tile
 constexpr int kChunk = 32;                               // K per stage: one 128-byte row of FP32
-constexpr int kStages = 3;
+constexpr int kStages = 2;
+constexpr int kParts = 3;                                // TF32 parts of an operand
+constexpr int kPackRow = kParts * 128;                   // floats per pack row
 constexpr uint32_t kOpBytes = kTile * kChunk * 4;        // one operand part of one stage (16 KB)
-constexpr uint32_t kStageBytes = 4 * kOpBytes;           // A hi, A lo, B hi, B lo
+constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A0, A1, A2, B0, B1, B2
 constexpr int kThreads = 192;                            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
-constexpr uint32_t kTmemCols = 2 * kTile;                // two FP32 accumulators of 128 columns
+constexpr uint32_t kTmemCols = 4 * kTile;                // two pairs (big, small) of FP32 accumulators
 constexpr size_t kBarBytes = 256;
 constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + 1024;  // + alignment slack
 
@@ -180,10 +184,10 @@ __device__ __forceinline__ Tile decode_tile(uint32_t t, uint32_t tiles_r, uint32
 
 // ---------------------------------------------------------------- pack --
 // Rows [r_start, m) of the panel's L21 (columns k0 .. k0 + kb - 1) and
-// columns [r_start, m) of its U12 (rows k0 .. k0 + kb - 1), split into TF32
-// hi / lo parts: pack[z][i][slot0 + k] = hi, pack[z][i][128 + slot0 + k] = lo
-// for k < 64 (zero for k >= kb).  Blocks [0, nA) take 128 rows of L21 each,
-// the rest 128 columns of U12; blockIdx.z selects the value set.
+// columns [r_start, m) of its U12 (rows k0 .. k0 + kb - 1), split into three
+// TF32 parts: pack[z][i][128 * p + slot0 + k] = part p, for k < 64 (zero for
+// k >= kb).  Blocks [0, nA) take 128 rows of L21 each, the rest 128 columns of
+// U12; blockIdx.z selects the value set.
 __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ val_base, uint64_t stride,
                                                     const uint32_t *__restrict__ doff, uint32_t m, uint32_t k0,
                                                     uint32_t kb, uint32_t slot0, uint32_t r_start, uint32_t nA,
@@ -204,28 +208,30 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
         if (row0 + r >= m) return;
 #pragma unroll
         for (int i = 0; i < 32; ++i) x[i] = sT[h * 32 + i][r];
-        dst = packA + (size_t(blockIdx.z) * m + row0 + r) * 256 + slot0 + h * 32;
+        dst = packA + (size_t(blockIdx.z) * m + row0 + r) * kPackRow + slot0 + h * 32;
     } else {
         const uint32_t j = r_start + (blockIdx.x - nA) * kTile + r;
         if (j >= m) return;
         const float *src = val + doff[j] + k0 + h * 32;
 #pragma unroll
         for (int i = 0; i < 32; ++i) x[i] = (h * 32 + i < kb) ? ld_cg(src + i) : 0.0f;
-        dst = packB + (size_t(blockIdx.z) * m + j) * 256 + slot0 + h * 32;
+        dst = packB + (size_t(blockIdx.z) * m + j) * kPackRow + slot0 + h * 32;
     }
 #pragma unroll
     for (int i = 0; i < 32; i += 4) {
-        float4 hi, lo;
-        hi.x = tf32_rna(x[i]);
-        hi.y = tf32_rna(x[i + 1]);
-        hi.z = tf32_rna(x[i + 2]);
-        hi.w = tf32_rna(x[i + 3]);
-        lo.x = tf32_rna(x[i] - hi.x);
-        lo.y = tf32_rna(x[i + 1] - hi.y);
-        lo.z = tf32_rna(x[i + 2] - hi.z);
-        lo.w = tf32_rna(x[i + 3] - hi.w);
-        *reinterpret_cast<float4 *>(dst + i) = hi;
-        *reinterpret_cast<float4 *>(dst + 128 + i) = lo;
+        float4 p0, p1, p2;
+        float *a0 = &p0.x, *a1 = &p1.x, *a2 = &p2.x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float v = x[i + u];
+            a0[u] = tf32_rna(v);
+            const float r1 = v - a0[u];  // exact
+            a1[u] = tf32_rna(r1);
+            a2[u] = tf32_rna(r1 - a1[u]);  // r1 - a1 exact, and at most 11 bits remain
+        }
+        *reinterpret_cast<float4 *>(dst + i) = p0;
+        *reinterpret_cast<float4 *>(dst + 128 + i) = p1;
+        *reinterpret_cast<float4 *>(dst + 256 + i) = p2;
     }
 }
 
@@ -292,11 +298,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                     uint8_t *st = smem + s * kStageBytes;
                     mbar_arrive_expect_tx(&full[s], kStageBytes);
-                    const int xh = int(kc * kChunk), xl = 128 + xh;
-                    tma_load_3d(st, &mapA, &full[s], xh, ya, zz);
-                    tma_load_3d(st + kOpBytes, &mapA, &full[s], xl, ya, zz);
-                    tma_load_3d(st + 2 * kOpBytes, &mapB, &full[s], xh, yb, zz);
-                    tma_load_3d(st + 3 * kOpBytes, &mapB, &full[s], xl, yb, zz);
+#pragma unroll
+                    for (int p = 0; p < kParts; ++p) {
+                        const int x = int(p * 128 + kc * kChunk);
+                        tma_load_3d(st + p * kOpBytes, &mapA, &full[s], x, ya, zz);
+                        tma_load_3d(st + (kParts + p) * kOpBytes, &mapB, &full[s], x, yb, zz);
+                    }
                 }
             }
             if (!ok) atomicOr(status, DEV_TIMEOUT);
@@ -321,18 +328,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d = tmem + a * kTile;
+                    const uint32_t d_big = tmem + a * 2 * kTile, d_small = d_big + kTile;
                     const uint32_t base = smem_addr(smem + s * kStageBytes);
 #pragma unroll
                     for (uint32_t k8 = 0; k8 < kChunk / 8; ++k8) {
                         const uint32_t off = k8 * 32;  // 8 TF32 values = 32 bytes along K
-                        const uint64_t ah = kmajor_sw128_desc(base + off);
-                        const uint64_t al = kmajor_sw128_desc(base + kOpBytes + off);
-                        const uint64_t bh = kmajor_sw128_desc(base + 2 * kOpBytes + off);
-                        const uint64_t bl = kmajor_sw128_desc(base + 3 * kOpBytes + off);
-                        tc_mma_tf32(d, al, bh, k8 != 0);
-                        tc_mma_tf32(d, ah, bl, 1);
-                        tc_mma_tf32(d, ah, bh, 1);
+                        uint64_t A[kParts], B[kParts];
+#pragma unroll
+                        for (int p = 0; p < kParts; ++p) {
+                            A[p] = kmajor_sw128_desc(base + p * kOpBytes + off);
+                            B[p] = kmajor_sw128_desc(base + (kParts + p) * kOpBytes + off);
+                        }
+                        const uint32_t acc = k8 != 0;
+                        tc_mma_tf32(d_small, A[2], B[0], acc);  // 2^-22 terms first
+                        tc_mma_tf32(d_small, A[1], B[1], 1);
+                        tc_mma_tf32(d_small, A[0], B[2], 1);
+                        tc_mma_tf32(d_small, A[1], B[0], 1);  // 2^-11 terms
+                        tc_mma_tf32(d_small, A[0], B[1], 1);
+                        tc_mma_tf32(d_big, A[0], B[0], acc);
                     }
                     tc_commit(&empty[s]);
                     tc_commit(&acc_full[a]);
@@ -392,10 +405,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc_fence_after();
+                const uint32_t lane_base = tmem + ((q * 32) << 16) + a * 2 * kTile;
 #pragma unroll
                 for (int cc = 0; cc < 4; ++cc) {
                     float acc[32];
-                    tc_ld32(tmem + ((q * 32) << 16) + a * kTile + cc * 32, acc);
+                    tc_ld32(lane_base + cc * 32, acc);  // big
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
+                    tc_ld32(lane_base + kTile + cc * 32, acc);  // small
 #pragma unroll
                     for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
                 }
@@ -444,8 +461,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 cudaError_t dense_tc_tensor_map(float *pack, uint32_t m, uint32_t batch, CUtensorMap *map) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
-    const cuuint64_t dims[3] = {256, m, batch};
-    const cuuint64_t strides[2] = {256 * sizeof(float), cuuint64_t(m) * 256 * sizeof(float)};
+    const cuuint64_t dims[3] = {cuuint64_t(kPackRow), m, batch};
+    const cuuint64_t strides[2] = {kPackRow * sizeof(float), cuuint64_t(m) * kPackRow * sizeof(float)};
     const cuuint32_t box[3] = {uint32_t(kChunk), uint32_t(kTile), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pack, dims, strides, box, estr,

@@ -1432,7 +1432,7 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     // allocated once per handle
     const bool tc = h->m && h->tune.dense_tc_min && h->m >= h->tune.dense_tc_min;
     if (tc && h->pack_m != h->m) {
-        const size_t pack_bytes = sizeof(float) * 256 * size_t(h->m) * h->batch;
+        const size_t pack_bytes = sizeof(float) * kDensePackRow * size_t(h->m) * h->batch;
         GLU_CUDA(h->d_packA.alloc(pack_bytes), "allocate tensor-core operand packs");
         GLU_CUDA(h->d_packB.alloc(pack_bytes), "allocate tensor-core operand packs");
         GLU_CUDA(dense_tc_tensor_map(h->d_packA.as<float>(), h->m, h->batch, &h->map_packA), "tensor map");

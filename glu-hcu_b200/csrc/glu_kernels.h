@@ -99,11 +99,12 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
                                 DenseRegion reg, cudaStream_t st);
 // The same update on the tensor cores (glu_dense_tc.cu): the panels' L21 rows
-// and U12 columns are first packed as TF32 hi/lo parts (pack[z][i][256], one
-// row per trailing row or column; the first panel of a pair in slots 0..63,
-// the second in 64..127), then tiles of the region are computed by tcgen05
-// from TMA loads of the packs.  dense_tc_tensor_map describes a pack buffer
-// of `batch` value sets for the loads.
+// and U12 columns are first packed as three TF32 parts (pack[z][i][384], one
+// row per trailing row or column, part p at 128 p; the first panel of a pair
+// in slots 0..63, the second in 64..127), then tiles of the region are
+// computed by tcgen05 from TMA loads of the packs.  dense_tc_tensor_map
+// describes a pack buffer of `batch` value sets for the loads.
+constexpr uint32_t kDensePackRow = 384;
 cudaError_t dense_tc_tensor_map(float *pack, uint32_t m, uint32_t batch, CUtensorMap *map);
 cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count, const uint32_t *doff, uint32_t m,
                               uint32_t k0, uint32_t kb, uint32_t slot0, float *packA, float *packB,

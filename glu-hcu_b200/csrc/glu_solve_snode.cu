@@ -116,7 +116,7 @@ __device__ __forceinline__ void sn_sweep_u_small(const DevPattern &P, const SnSw
 }
 }  // namespace
 
-__global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+__global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0) {
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
@@ -133,6 +133,17 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan
     __shared__ uint32_t sB[kSnMaxWidth];
     if (tid < w) sB[tid] = P.diag[s + tid];
     __syncthreads();
+    // This thread's L21 row and its target: they do not depend on x, so they
+    // are loaded before the dependency chain (and serve every right-hand side).
+    const uint32_t r = t * blockDim.x + tid;  // L21 row of this thread
+    float lr[kSnMaxWidth];
+    uint32_t target = 0;
+    if (r < m) {
+        target = __ldg(P.ridx + lbase + r);
+#pragma unroll
+        for (int c = 0; c < int(kSnMaxWidth); ++c)
+            lr[c] = uint32_t(c) < w ? __ldg(val + sB[c] + (l + 1 - (s + c)) + r) : 0.0f;
+    }
     // L11, strictly lower: L(s+k, s+c) at diag[s+c] + (k - c); eight loads in flight per thread
     for (uint32_t e0 = 0; e0 < w * kSnMaxWidth; e0 += 8 * 256) {
         float v[8];
@@ -148,9 +159,6 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan
         }
     }
     __syncthreads();
-    if (tid < w) sB[tid] += l + 1 - (s + tid);  // L21(r, c) at sB[c] + r
-    __syncthreads();
-    const uint32_t r = t * blockDim.x + tid;  // L21 row of this thread
     for (uint32_t q = 0; q < nrhs; ++q) {
         float *yq = y + size_t(q) * n;
         if (tid < 32) {
@@ -172,15 +180,10 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_l(DevPattern P, SnSweepPlan
         __syncthreads();
         if (r < m) {
             float acc = 0.0f;
-            for (uint32_t c0 = 0; c0 < w; c0 += 16) {
-                float v[16];
 #pragma unroll
-                for (int u = 0; u < 16; ++u) v[u] = (c0 + u < w) ? __ldg(val + sB[c0 + u] + r) : 0.0f;
-#pragma unroll
-                for (int u = 0; u < 16; ++u)
-                    if (c0 + u < w) acc = fmaf(v[u], xs[c0 + u], acc);
-            }
-            if (acc != 0.0f) atomicAdd(yq + __ldg(P.ridx + lbase + r), -acc);
+            for (int c = 0; c < int(kSnMaxWidth); ++c)
+                if (uint32_t(c) < w) acc = fmaf(lr[c], xs[c], acc);
+            if (acc != 0.0f) atomicAdd(yq + target, -acc);
         }
         __syncthreads();
     }
@@ -246,6 +249,32 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
     }
     __syncthreads();
     const uint32_t e0 = t * kSnSweepAbove, e1 = min(e0 + kSnSweepAbove, pre[w]);
+    // kSnSweepAbove / 256 entries above the block per thread: column, target
+    // and value do not depend on x, so they are loaded before the chain
+    constexpr int kPer = int(kSnSweepAbove / 256);
+    uint32_t ecol[kPer], etg[kPer];
+    float eval[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const uint32_t e = e0 + tid + u * 256;
+        ecol[u] = kSnMaxWidth;  // none
+        etg[u] = 0u;
+        eval[u] = 0.0f;
+        if (e < e1) {
+            uint32_t lo = 0, hi = w;  // last c with pre[c] <= e
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (pre[mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const uint32_t p = sC[lo] + (e - pre[lo]);
+            ecol[u] = lo;
+            etg[u] = __ldg(P.ridx + p);
+            eval[u] = __ldg(val + p);
+        }
+    }
     for (uint32_t q = 0; q < nrhs; ++q) {
         float *yq = y + size_t(q) * n;
         if (tid < 32) {
@@ -267,35 +296,12 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
             }
         }
         __syncthreads();
-        // kSnSweepAbove / 256 entries per thread: all loads first, then the atomics
-        constexpr int kPer = int(kSnSweepAbove / 256);
-        uint32_t tg[kPer];
-        float pv[kPer];
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
-            const uint32_t e = e0 + tid + u * 256;
-            tg[u] = 0xffffffffu;
-            pv[u] = 0.0f;
-            if (e < e1) {
-                uint32_t lo = 0, hi = w;  // last c with pre[c] <= e
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (pre[mid] <= e)
-                        lo = mid;
-                    else
-                        hi = mid;
-                }
-                const float xc = xs[lo];
-                if (xc != 0.0f) {
-                    const uint32_t p = sC[lo] + (e - pre[lo]);
-                    tg[u] = __ldg(P.ridx + p);
-                    pv[u] = __fmul_rn(__ldg(val + p), xc);
-                }
-            }
+            if (ecol[u] >= kSnMaxWidth) continue;
+            const float xc = xs[ecol[u]];
+            if (xc != 0.0f) atomicAdd(yq + etg[u], -__fmul_rn(eval[u], xc));
         }
-#pragma unroll
-        for (int u = 0; u < kPer; ++u)
-            if (tg[u] != 0xffffffffu) atomicAdd(yq + tg[u], -pv[u]);
         __syncthreads();
     }
 }
