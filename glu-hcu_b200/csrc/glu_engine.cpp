@@ -88,12 +88,12 @@ static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
 // Kernel kinds of glu_factor for the optional per-kernel profile.
 enum KernelKind {
     KK_PERT = 0, KK_LEVEL, KK_CHAIN, KK_SCALE, KK_DGATHER, KK_PANEL, KK_UPDATE, KK_DSCATTER, KK_CHECK,
-    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE, KK_PACK, KK_UPDATE_TC
+    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE, KK_PACK, KK_UPDATE_TC, KK_DIAG_INV
 };
 static const char *const kKindNames[GLU_KERNEL_KINDS] = {
     "k_colsum+k_pert_finish", "k_factor_level", "k_factor_chain", "k_scale_level", "k_dense_gather",
     "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_diag", "k_sn_panel",
-    "k_sn_update", "k_dense_pack", "k_dense_update_tc"};
+    "k_sn_update", "k_dense_pack", "k_dense_update_tc", "k_dense_diag_inv"};
 
 // Events around every launch of one glu_factor call, when enabled.
 struct KernelProfiler {
@@ -208,7 +208,7 @@ struct glu_handle_s {
     DevBuf d_src_lu, d_src_scale, d_a0_rptr, d_a0_cidx, d_a0_vmap, d_a0_cptr, d_a0_ridx, d_a0_ident, d_ax0;
     bool ax0_loaded = false;
     // work buffers
-    DevBuf d_status, d_pert, d_colmax, d_diag_scratch, d_counters, d_ticket, d_y, d_io32, d_b64,
+    DevBuf d_status, d_pert, d_colmax, d_diag_scratch, d_counters, d_ticket, d_flags, d_y, d_io32, d_b64,
         d_x64, d_r64, d_norms;
     uint32_t *h_status = nullptr;  // pinned
     double *h_norms = nullptr;     // pinned
@@ -221,6 +221,9 @@ struct glu_handle_s {
     // tensor-core dense update: TF32 hi/lo operand packs and their TMA maps
     // (allocated on the first factorization that uses them)
     DevBuf d_packA, d_packB;
+    // inverses of the dense tail's 64 x 64 diagonal blocks (L and U) per value
+    // set, for the dense triangular solves
+    DevBuf d_dinv;
     CUtensorMap map_packA{}, map_packB{};
     uint32_t pack_m = 0;
     uint32_t num_sms = 148;
@@ -964,6 +967,9 @@ Status read_status(glu_handle_s *h, cudaStream_t st, uint32_t *flags) {
     return GLU_OK;
 }
 
+// Floats of the dense tail's diagonal-block inverses of one value set.
+size_t dinv_per_set(const glu_handle_s *h) { return size_t((h->m + 63) / 64) * 2 * 64 * 64; }
+
 // The solve plan of the next solve: the handle's, with a pending
 // GLU_INJECT_UNSET_SOLVE_FLAG applied (and consumed).
 SolvePlanDev solve_plan(glu_handle_s *h) {
@@ -975,23 +981,33 @@ SolvePlanDev solve_plan(glu_handle_s *h) {
     return S;
 }
 
-// One FP32 solve of y in place (nrhs vectors of n), in the permuted system,
-// with the factors of value set z.
-Status solve_inplace(glu_handle_s *h, uint32_t z, float *y, uint32_t nrhs, bool trans, cudaStream_t st) {
-    uint32_t *cnt = h->d_counters.as<uint32_t>();
+// One FP32 solve of y in place (nrhs vectors of n per value set), in the
+// permuted system, with the factors of value sets [z, z + count).
+Status solve_inplace(glu_handle_s *h, uint32_t z, uint32_t count, float *y, uint32_t nrhs, bool trans,
+                     cudaStream_t st) {
+    const uint32_t nb = (h->m + 63) / 64 + 1;
+    GLU_CUDA(h->d_flags.ensure(sizeof(uint32_t) * size_t(nb) * count), "allocate solve flags");
+    GLU_CUDA(h->d_ticket.ensure(sizeof(uint32_t) * std::max<size_t>(count, 64)), "allocate solve flags");
+    uint32_t *cnt = h->d_flags.as<uint32_t>();
     uint32_t *tk = h->d_ticket.as<uint32_t>();
     uint32_t *status = h->d_status.as<uint32_t>();
     const float *val = h->d_val.as<float>() + size_t(z) * h->nnz;
     const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(z) * h->m * h->m : val;
-    GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs), "allocate solve buffer");
+    SolveBatch B;
+    B.count = count;
+    B.vstride = h->nnz;
+    B.dstride = h->dense_buffer ? uint64_t(h->m) * h->m : h->nnz;
+    B.dinv = h->m ? h->d_dinv.as<float>() + size_t(z) * dinv_per_set(h) : nullptr;
+    GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs * count), "allocate solve buffer");
     float *xo = h->d_xo.as<float>();
     const SolvePlanDev S = solve_plan(h);
     if (!trans) {
-        GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "lower solve");
-        GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "upper solve");
+        GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st), "lower solve");
+        GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st), "upper solve");
     } else {
-        GLU_CUDA(solve_upper_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st), "transposed upper solve");
-        GLU_CUDA(solve_lower_unit_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, st),
+        GLU_CUDA(solve_upper_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st),
+                 "transposed upper solve");
+        GLU_CUDA(solve_lower_unit_trans(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st),
                  "transposed lower solve");
     }
     return GLU_OK;
@@ -1018,7 +1034,7 @@ Status solve_f32(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, 
     const TransformDev &T = h->T;
     GLU_CUDA(launch_transform_f32(trans ? T.tin_idx : T.in_idx, trans ? T.tin_scale : T.in_scale, bin, y,
                                   h->n, nrhs, st), "transform");
-    Status s = solve_inplace(h, inst, y, nrhs, trans, st);
+    Status s = solve_inplace(h, inst, 1, y, nrhs, trans, st);
     if (s != GLU_OK) return s;
     float *xout = (where == GLU_HOST) ? io : x;
     GLU_CUDA(launch_transform_f32(trans ? T.tout_idx : T.out_idx, trans ? T.tout_scale : T.out_scale, y,
@@ -1059,8 +1075,10 @@ Status solve_f32_scratch(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const fl
     const float *dval = h->dense_buffer ? h->d_dense.as<float>() + size_t(inst) * h->m * h->m : val;
     uint32_t *status = h->d_status.as<uint32_t>();
     const SolvePlanDev S = solve_plan(h);
-    GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, st), "lower solve");
-    GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, st), "upper solve");
+    SolveBatch one;
+    one.dinv = h->m ? h->d_dinv.as<float>() + size_t(inst) * dinv_per_set(h) : nullptr;
+    GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, one, st), "lower solve");
+    GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, flags, ticket, status, one, st), "upper solve");
     GLU_CUDA(launch_transform_f32(T.out_idx, T.out_scale, y, x, h->n, nrhs, st), "transform");
     uint32_t fl = 0;
     Status s = read_status(h, st, &fl);
@@ -1522,6 +1540,13 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
         GLU_LAUNCH(KK_DSCATTER,
                    launch_dense_scatter(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
                    "factor (dense scatter)");
+    if (h->m) {
+        GLU_CUDA(h->d_dinv.ensure(sizeof(float) * dinv_per_set(h) * h->batch), "allocate diagonal-block inverses");
+        GLU_LAUNCH(KK_DIAG_INV,
+                   launch_dense_diag_inv(dbase, dstride, count, doff, h->m,
+                                         h->d_dinv.as<float>() + size_t(first) * dinv_per_set(h), st),
+                   "factor (diagonal-block inverses)");
+    }
     GLU_LAUNCH(KK_CHECK, launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
 #undef GLU_LAUNCH
     GLU_CUDA(cudaEventRecord(h->ev1, st), "event");
@@ -1565,20 +1590,25 @@ glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uin
     if (!h->has_source || !h->ax0_loaded)
         return set_error(GLU_ERR_STATE, "refinement needs the source matrix values (glu_load_source_values)");
     if (nrhs == 0) return GLU_OK;
+    if (uint64_t(nrhs) * count > 65535)
+        return set_error(GLU_ERR_UNSUPPORTED, "count * nrhs = %llu right-hand sides exceed 65,535 per call",
+                         (unsigned long long)nrhs * count);
     DeviceGuard g(h->device);
     cudaStream_t st = S_(stream);
     const uint32_t n = h->n;
-    const size_t len = size_t(n) * nrhs;
+    // every value set's right-hand sides together: nvec vectors of n
+    const uint32_t nvec = nrhs * count;
+    const size_t len = size_t(n) * nvec;
     GLU_CUDA(h->d_y.ensure(sizeof(float) * len), "allocate");
     GLU_CUDA(h->d_b64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
     GLU_CUDA(h->d_x64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
     GLU_CUDA(h->d_r64.ensure(sizeof(double) * len), "allocate");
-    GLU_CUDA(h->d_norms.ensure(sizeof(double) * 4 * nrhs), "allocate");
-    if (h->h_norms_cap < 4 * size_t(nrhs)) {
+    GLU_CUDA(h->d_norms.ensure(sizeof(double) * 4 * nvec), "allocate");
+    if (h->h_norms_cap < 4 * size_t(nvec)) {
         if (h->h_norms) cudaFreeHost(h->h_norms);
         h->h_norms = nullptr;
-        GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_norms), sizeof(double) * 4 * nrhs), "allocate pinned");
-        h->h_norms_cap = 4 * size_t(nrhs);
+        GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_norms), sizeof(double) * 4 * nvec), "allocate pinned");
+        h->h_norms_cap = 4 * size_t(nvec);
     }
     const TransformDev &T = h->T;
     const bool tr = transposed != 0;
@@ -1589,69 +1619,61 @@ glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uin
     const uint32_t *rptr = tr ? h->d_a0_cptr.as<uint32_t>() : h->d_a0_rptr.as<uint32_t>();
     const uint32_t *cidx = tr ? h->d_a0_ridx.as<uint32_t>() : h->d_a0_cidx.as<uint32_t>();
     const uint32_t *vmap = tr ? h->d_a0_ident.as<uint32_t>() : h->d_a0_vmap.as<uint32_t>();
-    glu_refine_stats agg{0, 0.0, 0.0};
-    bool converged_all = true;
     float *y = h->d_y.as<float>();
     double *r = h->d_r64.as<double>();
     double *norms = h->d_norms.as<double>();
-    for (uint32_t z = first; z < first + count; ++z) {
-        const size_t off = size_t(z - first) * len;
-        const double *bz;
-        double *xz;
-        if (where == GLU_HOST) {
-            GLU_CUDA(cudaMemcpyAsync(h->d_b64.p, b + off, sizeof(double) * len, cudaMemcpyHostToDevice, st), "copy b");
-            bz = h->d_b64.as<double>();
-            xz = h->d_x64.as<double>();
-        } else {
-            bz = b + off;
-            xz = x + off;
-        }
-        const double *ax0 = h->d_ax0.as<double>() + size_t(z) * h->nnz_src;
-        GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
-        GLU_CUDA(launch_norms(bz, n, nrhs, norms + 2 * nrhs, st), "norms");
-        // x0 = solve(b)
-        GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, bz, y, n, nrhs, st), "transform");
-        s = solve_inplace(h, z, y, nrhs, tr, st);
-        if (s != GLU_OK) return s;
-        GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 0, st), "transform");
-        uint32_t it = 0;
-        double worst2 = 0, worstinf = 0;
-        for (;; ++it) {
-            GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, n, bz, xz, r, nrhs, norms, st), "residual");
-            GLU_CUDA(cudaMemcpyAsync(h->h_norms, norms, sizeof(double) * 4 * nrhs, cudaMemcpyDeviceToHost, st),
-                     "read norms");
-            GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
-            worst2 = 0;
-            worstinf = 0;
-            for (uint32_t v = 0; v < nrhs; ++v) {
-                double bn2 = std::sqrt(h->h_norms[2 * nrhs + 2 * v]), bninf = h->h_norms[2 * nrhs + 2 * v + 1];
-                double rn2 = std::sqrt(h->h_norms[2 * v]), rninf = h->h_norms[2 * v + 1];
-                double rel2 = bn2 > 0 ? rn2 / bn2 : rn2, relinf = bninf > 0 ? rninf / bninf : rninf;
-                if (!(rel2 == rel2)) rel2 = INFINITY;
-                worst2 = std::max(worst2, rel2);
-                worstinf = std::max(worstinf, relinf);
-            }
-            if (worst2 <= tol || it >= maxit) break;
-            GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, r, y, n, nrhs, st), "transform");
-            s = solve_inplace(h, z, y, nrhs, tr, st);
-            if (s != GLU_OK) return s;
-            GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nrhs, 1, st), "transform");
-        }
-        if (where == GLU_HOST)
-            GLU_CUDA(cudaMemcpyAsync(x + off, xz, sizeof(double) * len, cudaMemcpyDeviceToHost, st), "copy x");
-        uint32_t flags = 0;
-        s = read_status(h, st, &flags);
-        if (s != GLU_OK) return s;
-        if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
-        agg.iterations = std::max(agg.iterations, it);
-        agg.residual = std::max(agg.residual, worst2);
-        agg.residual_inf = std::max(agg.residual_inf, worstinf);
-        if (!(worst2 <= tol)) converged_all = false;
+    const double *bz;
+    double *xz;
+    if (where == GLU_HOST) {
+        GLU_CUDA(cudaMemcpyAsync(h->d_b64.p, b, sizeof(double) * len, cudaMemcpyHostToDevice, st), "copy b");
+        bz = h->d_b64.as<double>();
+        xz = h->d_x64.as<double>();
+    } else {
+        bz = b;
+        xz = x;
     }
-    if (stats) *stats = agg;
-    if (!converged_all)
-        return set_error(GLU_ERR_NOT_CONVERGED, "refinement stopped at relative residual %.3e > %.3e",
-                         agg.residual, tol);
+    const double *ax0 = h->d_ax0.as<double>() + size_t(first) * h->nnz_src;
+    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
+    GLU_CUDA(launch_norms(bz, n, nvec, norms + 2 * nvec, st), "norms");
+    // x0 = solve(b), every value set at once
+    GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, bz, y, n, nvec, st), "transform");
+    s = solve_inplace(h, first, count, y, nrhs, tr, st);
+    if (s != GLU_OK) return s;
+    GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nvec, 0, st), "transform");
+    // r = b - A0 x, x += solve(r), with every value set in each step, until the
+    // worst relative residual of all right-hand sides meets tol
+    uint32_t it = 0;
+    double worst2 = 0, worstinf = 0;
+    for (;; ++it) {
+        GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, n, bz, xz, r, nvec, nrhs, h->nnz_src, norms, st), "residual");
+        GLU_CUDA(cudaMemcpyAsync(h->h_norms, norms, sizeof(double) * 4 * nvec, cudaMemcpyDeviceToHost, st),
+                 "read norms");
+        GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
+        worst2 = 0;
+        worstinf = 0;
+        for (uint32_t v = 0; v < nvec; ++v) {
+            double bn2 = std::sqrt(h->h_norms[2 * nvec + 2 * v]), bninf = h->h_norms[2 * nvec + 2 * v + 1];
+            double rn2 = std::sqrt(h->h_norms[2 * v]), rninf = h->h_norms[2 * v + 1];
+            double rel2 = bn2 > 0 ? rn2 / bn2 : rn2, relinf = bninf > 0 ? rninf / bninf : rninf;
+            if (!(rel2 == rel2)) rel2 = INFINITY;
+            worst2 = std::max(worst2, rel2);
+            worstinf = std::max(worstinf, relinf);
+        }
+        if (worst2 <= tol || it >= maxit) break;
+        GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, r, y, n, nvec, st), "transform");
+        s = solve_inplace(h, first, count, y, nrhs, tr, st);
+        if (s != GLU_OK) return s;
+        GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nvec, 1, st), "transform");
+    }
+    if (where == GLU_HOST)
+        GLU_CUDA(cudaMemcpyAsync(x, xz, sizeof(double) * len, cudaMemcpyDeviceToHost, st), "copy x");
+    uint32_t flags = 0;
+    s = read_status(h, st, &flags);
+    if (s != GLU_OK) return s;
+    if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
+    if (stats) *stats = glu_refine_stats{it, worst2, worstinf};
+    if (!(worst2 <= tol))
+        return set_error(GLU_ERR_NOT_CONVERGED, "refinement stopped at relative residual %.3e > %.3e", worst2, tol);
     return GLU_OK;
 }
 

@@ -185,6 +185,20 @@ struct SnSweepPlan {
 constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep
 constexpr uint32_t kSnSweepAbove = 1024;  // U entries per block of the U sweep
 
+// Value sets solved together: set z uses the factors at val + z * vstride
+// (dense tail at dval + z * dstride) and the right-hand sides
+// [z * nrhs, (z + 1) * nrhs) of the vectors (contiguous, n each).
+struct SolveBatch {
+    uint32_t count = 1;
+    uint64_t vstride = 0;
+    uint64_t dstride = 0;
+    const float *dinv = nullptr;  // inverses of the dense tail's diagonal blocks of the first set
+};
+// Inverses of the 64 x 64 diagonal blocks of the dense tail's L and U, per
+// value set: dinv[z][b][0: L, 1: U][64 x 64] (row-major), from the factors.
+cudaError_t launch_dense_diag_inv(const float *dval, uint64_t dstride, uint32_t count, const uint32_t *doff,
+                                  uint32_t m, float *dinv, cudaStream_t st);
+
 struct SolvePlanDev {
     uint32_t t;                     // first column of the dense tail (n if none)
     uint32_t m;                     // order of the dense tail
@@ -202,7 +216,7 @@ struct SolvePlanDev {
 // Supernodal sweep over the columns [0, t) (forward L, or backward U), then
 // y[0, t) = xo[0, t).
 cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
-                         float *y, float *xo, uint32_t nrhs, cudaStream_t st);
+                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, cudaStream_t st);
 
 // Transform in: y[j] = rhs[col_perm[piv[j]]] * (mc64 ? col_scale_perm[piv[j]] : 1)
 // (symbolic.cc:215-223); out: x[j] = y[row_perm_inv[j]] * (mc64 ? row_scale[j] : 1)
@@ -219,23 +233,24 @@ struct TransformDev {
 };
 
 constexpr uint32_t kSolveChainThreads = 512;
-// FP32 triangular solves on y (nrhs vectors of n, one after another), in
-// place.  val: CSC factor values; dval: base of the dense tail view.
-// xo: n * nrhs floats of scratch (finished values of the dividing sweeps);
-// counters / ticket: scratch of the dense tail sweeps.
+// FP32 triangular solves on y (nrhs vectors of n per value set, one after
+// another, B.count value sets), in place.  val: CSC factor values; dval: base
+// of the dense tail view.  xo: scratch of y's size (finished values of the
+// dividing sweeps); counters / ticket: scratch of the dense tail sweeps
+// (B.count * (m / 64 + 1) flags, B.count tickets).
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                             uint32_t *ticket, uint32_t *status, cudaStream_t st);
+                             uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st);
 cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val,
                         const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                        uint32_t *ticket, uint32_t *status, cudaStream_t st);
+                        uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st);
 // Transposed: U^T z = y (forward), then L^T w = z (backward).
 cudaError_t solve_upper_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
                               const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                              uint32_t *ticket, uint32_t *status, cudaStream_t st);
+                              uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st);
 cudaError_t solve_lower_unit_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
                                    const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                                   uint32_t *ticket, uint32_t *status, cudaStream_t st);
+                                   uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st);
 
 // Permute/scale kernels of the solve transforms.
 cudaError_t launch_transform_f32(const uint32_t *idx, const double *scale, const float *in,
@@ -247,10 +262,12 @@ cudaError_t launch_transform_f32_to_f64_add(const uint32_t *idx, const double *s
                                             int accumulate, cudaStream_t st);
 
 // FP64 residual r = b - A0 x (or A0^T) per right-hand side, with per-vector
-// sums of squares and max-abs accumulated into norms[2*v + {0,1}].
+// sums of squares and max-abs accumulated into norms[2*v + {0,1}].  nvec
+// vectors; vector v uses the A0 values ax0 + (v / nrhs_per_set) * ax0_stride.
 cudaError_t launch_residual(const uint32_t *a_rptr, const uint32_t *a_cidx, const uint32_t *a_vmap,
                             const double *ax0, uint32_t n, const double *b, const double *x,
-                            double *r, uint32_t nrhs, double *norms, cudaStream_t st);
+                            double *r, uint32_t nvec, uint32_t nrhs_per_set, uint64_t ax0_stride,
+                            double *norms, cudaStream_t st);
 cudaError_t launch_norms(const double *v, uint32_t n, uint32_t nvec, double *norms,
                          cudaStream_t st);
 

@@ -20,6 +20,8 @@
 //    is one parallel scatter or gather over the tail columns.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 
@@ -102,7 +104,10 @@ template <int kMode>
 __global__ void __launch_bounds__(256) k_sweep_level(DevPattern P, const float *__restrict__ val, float *y, float *xo,
                                                      uint32_t nrhs, const uint32_t *__restrict__ cols,
                                                      const uint32_t *__restrict__ item_off, uint32_t s0,
-                                                     uint32_t s1) {
+                                                     uint32_t s1, uint64_t vstride, uint64_t ystride) {
+    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
+    y += blockIdx.z * ystride;
+    xo += blockIdx.z * ystride;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
     const uint32_t it0 = item_off[s0], it1 = item_off[s1];
@@ -118,7 +123,11 @@ __global__ void __launch_bounds__(kSolveChainThreads) k_sweep_chain(DevPattern P
                                                                     const uint32_t *__restrict__ cols,
                                                                     const uint32_t *__restrict__ lptr,
                                                                     const uint32_t *__restrict__ item_off,
-                                                                    uint32_t l0, uint32_t l1) {
+                                                                    uint32_t l0, uint32_t l1, uint64_t vstride,
+                                                                    uint64_t ystride) {
+    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
+    y += blockIdx.z * ystride;
+    xo += blockIdx.z * ystride;
     cg::cluster_group cluster = cg::this_cluster();
     const uint32_t nblk = cluster.num_blocks();
     const uint32_t rank = cluster.block_rank();
@@ -141,7 +150,10 @@ __global__ void __launch_bounds__(kSolveChainThreads) k_sweep_chain(DevPattern P
 template <bool kRow>
 __global__ void __launch_bounds__(256) k_tail_coupling(DevPattern P, uint32_t t, uint32_t m,
                                                        const uint32_t *__restrict__ tail_start,
-                                                       const float *__restrict__ val, float *y, uint32_t nrhs) {
+                                                       const float *__restrict__ val, float *y, uint32_t nrhs,
+                                                       uint64_t vstride, uint64_t ystride) {
+    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
+    y += blockIdx.z * ystride;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t jj = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (jj >= m) return;
@@ -167,15 +179,19 @@ __global__ void k_copy_sparse(const float *__restrict__ xo, float *y, uint32_t t
 
 template <int kMode>
 static cudaError_t run_sweep(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y, float *xo,
-                             uint32_t nrhs, cudaStream_t st) {
+                             uint32_t nrhs, const SolveBatch &B, cudaStream_t st) {
     const SweepPlan &sw = S.sweep[kMode];
+    const uint64_t ystride = uint64_t(nrhs) * P.n;
+    // blocks per value set of a wide level: about eight per SM in all
+    const uint32_t wide_blocks = std::max<uint32_t>(1u, (148u * 8u + B.count - 1) / B.count);
     for (uint32_t i = 0; i < sw.nsteps; ++i) {
         const SweepStep &s = sw.steps[i];
         if (s.kind == 0) {
-            k_sweep_level<kMode><<<148 * 8, 256, 0, st>>>(P, val, y, xo, nrhs, sw.cols, sw.item_off, s.s0, s.s1);
+            k_sweep_level<kMode><<<dim3(wide_blocks, 1, B.count), 256, 0, st>>>(
+                P, val, y, xo, nrhs, sw.cols, sw.item_off, s.s0, s.s1, B.vstride, ystride);
         } else {
             cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(S.cluster, 1, 1);
+            cfg.gridDim = dim3(S.cluster, 1, B.count);
             cfg.blockDim = dim3(kSolveChainThreads, 1, 1);
             cfg.stream = st;
             cudaLaunchAttribute attr[1];
@@ -186,14 +202,14 @@ static cudaError_t run_sweep(const DevPattern &P, const SolvePlanDev &S, const f
             cfg.attrs = attr;
             cfg.numAttrs = 1;
             cudaError_t e = cudaLaunchKernelEx(&cfg, k_sweep_chain<kMode>, P, val, y, xo, nrhs, sw.cols, sw.lptr,
-                                               sw.item_off, s.l0, s.l1);
+                                               sw.item_off, s.l0, s.l1, B.vstride, ystride);
             if (e != cudaSuccess) return e;
         }
     }
     if ((kMode == SWEEP_U || kMode == SWEEP_UT) && S.t > 0) {
         uint32_t bx = (S.t + 255) / 256;
         if (bx > 1024) bx = 1024;
-        k_copy_sparse<<<dim3(bx, nrhs, 1), 256, 0, st>>>(xo, y, S.t, P.n);
+        k_copy_sparse<<<dim3(bx, nrhs * B.count, 1), 256, 0, st>>>(xo, y, S.t, P.n);
     }
     return cudaGetLastError();
 }
@@ -205,24 +221,71 @@ static cudaError_t run_sweep(const DevPattern &P, const SolvePlanDev &S, const f
 //   kMode 2: T = U^T (lower,           T(i,c) = val[doff[i] + c])
 //   kMode 3: T = L^T (unit upper,      T(i,c) = val[doff[i] + c])
 // Row blocks of 64 are claimed in solve order (ascending for lower, descending
-// for upper); flags[b] = 1 once block b is solved.
+// for upper); flags[b] = 1 once block b is solved.  The diagonal block's
+// solve is a product with its inverse (dinv, computed once per factorization
+// by k_dense_diag_inv), so the step between two blocks of the chain is a
+// parallel 64 x 64 mat-vec instead of 64 dependent substitution steps.
 constexpr int kRB = 64;
 constexpr int kRHSChunk = 4;
+
+// Inverses of the 64 x 64 diagonal blocks of the dense tail: blockIdx.y = 0
+// the unit lower L_bb, 1 the upper U_bb; dinv[z][b][which] row-major.  Thread
+// j computes column j by substitution (rows past the tail's end are the
+// identity).  blockIdx.z selects the value set.
+__global__ void __launch_bounds__(kRB) k_dense_diag_inv(const float *__restrict__ val, uint64_t dstride,
+                                                         const uint32_t *__restrict__ doff, uint32_t m,
+                                                         float *__restrict__ dinv) {
+    __shared__ float T[kRB][kRB + 1];
+    __shared__ float X[kRB][kRB + 1];
+    const uint32_t b = blockIdx.x, which = blockIdx.y, j = threadIdx.x;
+    const uint32_t nb = (m + kRB - 1) / kRB;
+    val += blockIdx.z * dstride;
+    const uint32_t rb0 = b * kRB, rows = min(uint32_t(kRB), m - rb0);
+    for (uint32_t e = j; e < uint32_t(kRB * kRB); e += kRB) {
+        const uint32_t c = e / kRB, i = e % kRB;
+        T[i][c] = (i < rows && c < rows) ? val[doff[rb0 + c] + rb0 + i] : (i == c ? 1.0f : 0.0f);
+    }
+    __syncthreads();
+    if (which == 0) {  // unit lower: X(:, j) = L^-1 e_j
+        for (uint32_t i = 0; i < uint32_t(kRB); ++i) X[i][j] = i == j ? 1.0f : 0.0f;
+        for (uint32_t i = j + 1; i < uint32_t(kRB); ++i) {
+            float acc = 0.0f;
+            for (uint32_t k = j; k < i; ++k) acc = fmaf(T[i][k], X[k][j], acc);
+            X[i][j] = -acc;
+        }
+    } else {  // upper: X(:, j) = U^-1 e_j
+        for (uint32_t i = 0; i < uint32_t(kRB); ++i) X[i][j] = 0.0f;
+        X[j][j] = 1.0f / T[j][j];
+        for (uint32_t i = j; i-- > 0;) {
+            float acc = 0.0f;
+            for (uint32_t k = i + 1; k <= j; ++k) acc = fmaf(T[i][k], X[k][j], acc);
+            X[i][j] = -acc / T[i][i];
+        }
+    }
+    float *out = dinv + ((size_t(blockIdx.z) * nb + b) * 2 + which) * kRB * kRB;
+    for (uint32_t i = 0; i < uint32_t(kRB); ++i) out[i * kRB + j] = X[i][j];
+}
 
 template <int kMode>
 __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ val, const uint32_t *__restrict__ doff,
                                                     uint32_t t, uint32_t m, float *y, uint32_t n, uint32_t nrhs,
                                                     uint32_t *flags, uint32_t *ticket, uint32_t *status,
-                                                    uint32_t spin_limit, uint32_t ticket_base) {
+                                                    uint32_t spin_limit, uint32_t ticket_base, uint64_t dstride,
+                                                    uint64_t ystride, const float *__restrict__ dinv) {
     constexpr bool kLower = (kMode == 0 || kMode == 2);
     constexpr bool kTrans = (kMode >= 2);
-    constexpr bool kUnit = (kMode == 0 || kMode == 3);
+    constexpr int kWhich = (kMode == 0 || kMode == 3) ? 0 : 1;  // inverse of L or of U
     __shared__ float tile[kRB][kRB + 1];
     __shared__ float xs[kRB][kRHSChunk];
     __shared__ float part[4][kRB][kRHSChunk];
     __shared__ uint32_t s_blk;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = (m + kRB - 1) / kRB;
+    // value set blockIdx.z: its factors, right-hand sides, block flags, ticket
+    val += blockIdx.z * dstride;
+    y += blockIdx.z * ystride;
+    flags += size_t(blockIdx.z) * nb;
+    ticket += blockIdx.z;
     if (tid == 0) s_blk = atomicAdd(ticket, 1u) + ticket_base;
     __syncthreads();
     const uint32_t tk = s_blk;
@@ -233,15 +296,13 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     auto T = [&](uint32_t i, uint32_t c) -> float {
         return kTrans ? val[doff[i] + c] : val[doff[c] + i];
     };
-    // the diagonal tile does not depend on x either: its loads are issued first
+    // the diagonal block's inverse does not depend on x either: its loads are
+    // issued first (row-major; transposed for the transposed sweeps)
     constexpr int kTilePer = kRB * kRB / 256;
     float dv[kTilePer];
+    const float *inv = dinv + ((size_t(blockIdx.z) * nb + b) * 2 + kWhich) * kRB * kRB;
 #pragma unroll
-    for (int qq = 0; qq < kTilePer; ++qq) {
-        const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
-        const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
-        dv[qq] = (rb0 + i < rb1 && rb0 + cc < rb1) ? T(rb0 + i, rb0 + cc) : 0.0f;
-    }
+    for (int qq = 0; qq < kTilePer; ++qq) dv[qq] = __ldg(inv + tid + qq * 256);
     for (uint32_t rc0 = 0; rc0 < nrhs; rc0 += kRHSChunk) {
         const uint32_t nr = min(uint32_t(kRHSChunk), nrhs - rc0);
         const uint32_t row = tid & (kRB - 1), q = tid / kRB;  // 4 quarters of 16 columns
@@ -286,44 +347,42 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
         }
 #pragma unroll
         for (int r = 0; r < kRHSChunk; ++r) part[q][row][r] = acc[r];
-        // diagonal tile (its loads were issued at the start)
+        // r = y - (contributions) for the block's rows, then x = T_bb^-1 r
 #pragma unroll
         for (int qq = 0; qq < kTilePer; ++qq) {
-            const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
-            const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
-            tile[i][cc] = dv[qq];
+            const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;  // inverse element (a, bb)
+            if (kTrans)
+                tile[bb][a] = dv[qq];
+            else
+                tile[a][bb] = dv[qq];
         }
         __syncthreads();
-        // one warp per right-hand side solves the diagonal tile
-        const uint32_t w = tid >> 5, lane = tid & 31;
-        if (w < nr) {
-            const uint32_t r = w;
-            float v0 = 0.f, v1 = 0.f;  // rows lane and lane+32
-            if (lane < rows)
-                v0 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane) -
-                     (part[0][lane][r] + part[1][lane][r] + part[2][lane][r] + part[3][lane][r]);
-            if (lane + 32 < rows)
-                v1 = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + lane + 32) -
-                     (part[0][lane + 32][r] + part[1][lane + 32][r] + part[2][lane + 32][r] + part[3][lane + 32][r]);
-            for (uint32_t s = 0; s < rows; ++s) {
-                const uint32_t c = kLower ? s : rows - 1 - s;
-                float xc = __shfl_sync(0xffffffffu, c < 32 ? v0 : v1, c & 31);
-                if (!kUnit) xc = xc / tile[c][c];
-                if (lane == (c & 31)) {
-                    if (c < 32)
-                        v0 = xc;
-                    else
-                        v1 = xc;
-                }
-                // update the rows still to solve
-                uint32_t i0 = lane, i1 = lane + 32;
-                bool pend0 = kLower ? (i0 > c) : (i0 < c);
-                bool pend1 = kLower ? (i1 > c) : (i1 < c);
-                if (pend0 && i0 < rows) v0 -= tile[i0][c] * xc;
-                if (pend1 && i1 < rows) v1 -= tile[i1][c] * xc;
+        if (tid < kRB * kRHSChunk) {
+            const uint32_t i = tid % kRB, r = tid / kRB;
+            float v = 0.0f;
+            if (i < rows && r < nr)
+                v = __ldcg(y + size_t(rc0 + r) * n + t + rb0 + i) -
+                    (part[0][i][r] + part[1][i][r] + part[2][i][r] + part[3][i][r]);
+            xs[i][r] = v;
+        }
+        __syncthreads();
+        {
+            float acc2[kRHSChunk] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+            for (uint32_t cc = q * 16; cc < q * 16 + 16; ++cc) {
+                const float tv = tile[row][cc];
+#pragma unroll
+                for (int r = 0; r < kRHSChunk; ++r) acc2[r] = fmaf(tv, xs[cc][r], acc2[r]);
             }
-            if (lane < rows) __stcg(y + size_t(rc0 + r) * n + t + rb0 + lane, v0);
-            if (lane + 32 < rows) __stcg(y + size_t(rc0 + r) * n + t + rb0 + lane + 32, v1);
+#pragma unroll
+            for (int r = 0; r < kRHSChunk; ++r) part[q][row][r] = acc2[r];
+        }
+        __syncthreads();
+        if (tid < kRB * kRHSChunk) {
+            const uint32_t i = tid % kRB, r = tid / kRB;
+            if (i < rows && r < nr)
+                __stcg(y + size_t(rc0 + r) * n + t + rb0 + i,
+                       (part[0][i][r] + part[1][i][r]) + (part[2][i][r] + part[3][i][r]));
         }
         __syncthreads();
     }
@@ -333,65 +392,74 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     }
 }
 
+cudaError_t launch_dense_diag_inv(const float *dval, uint64_t dstride, uint32_t count, const uint32_t *doff,
+                                  uint32_t m, float *dinv, cudaStream_t st) {
+    if (m == 0) return cudaSuccess;
+    k_dense_diag_inv<<<dim3((m + kRB - 1) / kRB, 2, count), kRB, 0, st>>>(dval, dstride, doff, m, dinv);
+    return cudaGetLastError();
+}
+
 template <int kMode>
 static cudaError_t dense_sweep(const SolvePlanDev &S, const float *dval, float *y, uint32_t n,
                                uint32_t nrhs, uint32_t *flags, uint32_t *ticket, uint32_t *status,
-                               cudaStream_t st) {
+                               const SolveBatch &B, cudaStream_t st) {
     if (S.m == 0) return cudaSuccess;
     uint32_t nb = (S.m + kRB - 1) / kRB;
-    cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * nb, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
+    cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * nb * B.count, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t) * B.count, st);
     if (e != cudaSuccess) return e;
-    k_dense_trsv<kMode><<<nb, 256, 0, st>>>(dval, S.doff, S.t, S.m, y, n, nrhs, flags, ticket, status,
-                                            S.spin_limit, S.ticket_base);
+    k_dense_trsv<kMode><<<dim3(nb, 1, B.count), 256, 0, st>>>(dval, S.doff, S.t, S.m, y, n, nrhs, flags, ticket,
+                                                              status, S.spin_limit, S.ticket_base, B.dstride,
+                                                              uint64_t(nrhs) * n, B.dinv);
     return cudaGetLastError();
 }
 
 static cudaError_t tail_coupling(const DevPattern &P, const SolvePlanDev &S, const float *val, float *y,
-                                 uint32_t nrhs, bool rows, cudaStream_t st) {
+                                 uint32_t nrhs, bool rows, const SolveBatch &B, cudaStream_t st) {
     if (S.m == 0 || S.t == 0) return cudaSuccess;
-    uint32_t blocks = (S.m + 7) / 8;
+    const dim3 grid((S.m + 7) / 8, 1, B.count);
+    const uint64_t ystride = uint64_t(nrhs) * P.n;
     if (rows)
-        k_tail_coupling<true><<<blocks, 256, 0, st>>>(P, S.t, S.m, S.tail_row_start, val, y, nrhs);
+        k_tail_coupling<true><<<grid, 256, 0, st>>>(P, S.t, S.m, S.tail_row_start, val, y, nrhs, B.vstride, ystride);
     else
-        k_tail_coupling<false><<<blocks, 256, 0, st>>>(P, S.t, S.m, S.tail_start, val, y, nrhs);
+        k_tail_coupling<false><<<grid, 256, 0, st>>>(P, S.t, S.m, S.tail_start, val, y, nrhs, B.vstride, ystride);
     return cudaGetLastError();
 }
 
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                             uint32_t *ticket, uint32_t *status, cudaStream_t st) {
-    cudaError_t e = S.sn[0].nlev ? run_sn_sweep(P, S.sn[0], false, S.t, val, y, xo, nrhs, st)
-                                 : run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, st);
+                             uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st) {
+    cudaError_t e = S.sn[0].nlev ? run_sn_sweep(P, S.sn[0], false, S.t, val, y, xo, nrhs, B, st)
+                                 : run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, B, st);
     if (e != cudaSuccess) return e;
-    return dense_sweep<0>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
+    return dense_sweep<0>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
 }
 
 cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float *val,
                         const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                        uint32_t *ticket, uint32_t *status, cudaStream_t st) {
-    cudaError_t e = dense_sweep<1>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
-    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, false, st);
+                        uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st) {
+    cudaError_t e = dense_sweep<1>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
+    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, false, B, st);
     if (e == cudaSuccess)
-        e = S.sn[1].nlev ? run_sn_sweep(P, S.sn[1], true, S.t, val, y, xo, nrhs, st)
-                         : run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, st);
+        e = S.sn[1].nlev ? run_sn_sweep(P, S.sn[1], true, S.t, val, y, xo, nrhs, B, st)
+                         : run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, B, st);
     return e;
 }
 
 cudaError_t solve_upper_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
                               const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                              uint32_t *ticket, uint32_t *status, cudaStream_t st) {
-    cudaError_t e = run_sweep<SWEEP_UT>(P, S, val, y, xo, nrhs, st);
-    if (e == cudaSuccess) e = dense_sweep<2>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
+                              uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st) {
+    cudaError_t e = run_sweep<SWEEP_UT>(P, S, val, y, xo, nrhs, B, st);
+    if (e == cudaSuccess) e = dense_sweep<2>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
     return e;
 }
 
 cudaError_t solve_lower_unit_trans(const DevPattern &P, const SolvePlanDev &S, const float *val,
                                    const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
-                                   uint32_t *ticket, uint32_t *status, cudaStream_t st) {
-    cudaError_t e = dense_sweep<3>(S, dval, y, P.n, nrhs, counters, ticket, status, st);
-    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, true, st);
-    if (e == cudaSuccess) e = run_sweep<SWEEP_LT>(P, S, val, y, xo, nrhs, st);
+                                   uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st) {
+    cudaError_t e = dense_sweep<3>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
+    if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, true, B, st);
+    if (e == cudaSuccess) e = run_sweep<SWEEP_LT>(P, S, val, y, xo, nrhs, B, st);
     return e;
 }
 
@@ -457,10 +525,11 @@ __global__ void __launch_bounds__(256) k_residual(const uint32_t *__restrict__ r
                                                   const uint32_t *__restrict__ vmap, const double *__restrict__ ax0,
                                                   uint32_t n, const double *__restrict__ b,
                                                   const double *__restrict__ x, double *__restrict__ r,
-                                                  double *norms) {
+                                                  double *norms, uint32_t nrhs_per_set, uint64_t ax0_stride) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t v = blockIdx.y;
     const size_t off = size_t(v) * n;
+    ax0 += (v / nrhs_per_set) * ax0_stride;  // the value set of vector v
     double ss = 0.0, mx = 0.0;
     for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) / 32; row < n;
          row += gridDim.x * blockDim.x / 32) {
@@ -485,12 +554,16 @@ __global__ void __launch_bounds__(256) k_residual(const uint32_t *__restrict__ r
 
 cudaError_t launch_residual(const uint32_t *a_rptr, const uint32_t *a_cidx, const uint32_t *a_vmap,
                             const double *ax0, uint32_t n, const double *b, const double *x,
-                            double *r, uint32_t nrhs, double *norms, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st);
+                            double *r, uint32_t nvec, uint32_t nrhs_per_set, uint64_t ax0_stride,
+                            double *norms, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nvec, st);
     if (e != cudaSuccess) return e;
     uint32_t blocks = (n + 7) / 8;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    k_residual<<<dim3(blocks, nrhs, 1), 256, 0, st>>>(a_rptr, a_cidx, a_vmap, ax0, n, b, x, r, norms);
+    // about eight blocks per SM in all
+    const uint32_t cap = std::max<uint32_t>(1u, (148u * 8u + nvec - 1) / nvec);
+    if (blocks > cap) blocks = cap;
+    k_residual<<<dim3(blocks, nvec, 1), 256, 0, st>>>(a_rptr, a_cidx, a_vmap, ax0, n, b, x, r, norms,
+                                                      std::max<uint32_t>(nrhs_per_set, 1u), ax0_stride);
     return cudaGetLastError();
 }
 

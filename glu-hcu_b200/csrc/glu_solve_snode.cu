@@ -117,7 +117,11 @@ __device__ __forceinline__ void sn_sweep_u_small(const DevPattern &P, const SnSw
 }  // namespace
 
 __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
-                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0) {
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0,
+                                                    uint64_t vstride, uint64_t ystride) {
+    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
+    y += blockIdx.z * ystride;
+    xo += blockIdx.z * ystride;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     const uint2 bi = W.map[b0 + blockIdx.x];
@@ -190,7 +194,11 @@ __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan
 }
 
 __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
-                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0) {
+                                                    float *y, float *xo, uint32_t nrhs, uint32_t b0,
+                                                    uint64_t vstride, uint64_t ystride) {
+    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
+    y += blockIdx.z * ystride;
+    xo += blockIdx.z * ystride;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     __shared__ uint32_t pre[kSnMaxWidth + 1];
@@ -312,19 +320,21 @@ __global__ void k_sn_copy(const float *__restrict__ xo, float *y, uint32_t t, ui
 }
 
 cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
-                         float *y, float *xo, uint32_t nrhs, cudaStream_t st) {
+                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, cudaStream_t st) {
+    const uint64_t ystride = uint64_t(nrhs) * P.n;
     for (uint32_t l = 0; l < W.nlev; ++l) {
         const SnSweepLevel &lv = W.levels[l];
         if (lv.blocks == 0) continue;
+        const dim3 grid(lv.blocks, 1, B.count);
         if (upper)
-            k_sn_sweep_u<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0);
+            k_sn_sweep_u<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride);
         else
-            k_sn_sweep_l<<<lv.blocks, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0);
+            k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride);
     }
-    if (t > 0) {
+    if (t > 0) {  // the vectors of all value sets are contiguous: nrhs * count of them
         uint32_t bx = (t + 255) / 256;
         if (bx > 1024) bx = 1024;
-        k_sn_copy<<<dim3(bx, nrhs, 1), 256, 0, st>>>(xo, y, t, P.n);
+        k_sn_copy<<<dim3(bx, nrhs * B.count, 1), 256, 0, st>>>(xo, y, t, P.n);
     }
     return cudaGetLastError();
 }

@@ -40,7 +40,7 @@ ENGINE_SYMBOLS = [
     "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
     "glu_kernel_kind_name", "glu_measure_fp32_peak", "glu_set_wait_limit", "glu_debug_inject",
 ]
-GLU_KERNEL_KINDS = 14
+GLU_KERNEL_KINDS = 15
 PRE_SYMBOLS = [
     "glu_pre_analyze", "glu_pre_n", "glu_pre_nnz", "glu_pre_matrix", "glu_pre_transform",
     "glu_pre_source_map", "glu_pre_destroy", "glu_pre_read_mtx", "glu_pre_free",

@@ -218,7 +218,7 @@ glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
  * summed milliseconds and launch counts of the last glu_factor call (arrays
  * of GLU_KERNEL_KINDS entries; see glu_kernel_kind_name).  Off by default:
  * the events add a little time between launches. */
-#define GLU_KERNEL_KINDS 14
+#define GLU_KERNEL_KINDS 15
 glu_status glu_profile_enable(glu_handle_t h, int on);
 glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
 const char *glu_kernel_kind_name(int kind);
