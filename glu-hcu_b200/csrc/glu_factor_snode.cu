@@ -419,6 +419,23 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
     const uint32_t w = d.w;
     const uint32_t nrt = (d.m + kTile - 1) / kTile;
     const uint32_t r0 = (t % nrt) * kTile, c0 = (t / nrt) * kTile;
+    const uint32_t tr = tid & 15, tc = tid >> 4;
+    // Target positions from the table depend only on the tile: issued first,
+    // in flight while the metadata and the operands are staged (a target that
+    // cannot hold the rows has 0xffffffff in the table).
+    uint32_t pos[4][4];
+    if (S.pos) {
+        const uint32_t *tab = S.pos + S.pos_off[i] + r0 + tr * 4;
+#pragma unroll
+        for (int bb = 0; bb < 4; ++bb) {
+            const uint32_t jt = tc * 4 + bb;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const uint32_t r = r0 + tr * 4 + a;
+                pos[a][bb] = (c0 + jt < d.nt && r < d.m) ? __ldg(tab + uint64_t(c0 + jt) * d.m + a) : 0xffffffffu;
+            }
+        }
+    }
     if (tid < w) sOff[tid] = P.diag[d.s + tid] + (d.l + 1 - (d.s + tid)) + r0;
     if (tid < kTile) {
         const uint32_t jt = c0 + tid;
@@ -442,22 +459,8 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
         const uint32_t jt = e / w, k = e - jt * w;
         sU[k][jt] = (k + sLen[jt] >= w) ? ld_cg(val + sPl[jt] - (w - 1 - k)) : 0.0f;
     }
-    const uint32_t tr = tid & 15, tc = tid >> 4;
-    uint32_t pos[4][4];
     float acc[4][4];
-    if (S.pos) {
-        const uint32_t *tab = S.pos + S.pos_off[i] + r0 + tr * 4;
-#pragma unroll
-        for (int bb = 0; bb < 4; ++bb) {
-            const uint32_t jt = tc * 4 + bb;
-            const bool tv = sLen[jt] != 0;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const uint32_t r = r0 + tr * 4 + a;
-                pos[a][bb] = (tv && r < d.m) ? __ldg(tab + uint64_t(c0 + jt) * d.m + a) : 0xffffffffu;
-            }
-        }
-    } else {
+    if (!S.pos) {
         uint32_t rowid[4];
         const uint32_t lbase = P.diag[d.l] + 1;
 #pragma unroll
