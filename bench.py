@@ -48,10 +48,11 @@ def parse():
     p.add_argument("--no-batch-record", action="store_true",
                    help="skip the batched same-pattern sub-record of the mesh line")
     p.add_argument("--side", type=int, default=700, help="mesh side (workload mesh)")
+    p.add_argument("--batch", type=int, default=256, help="value sets of the batch workload")
     return p.parse_args()
 
 
-def workload(name, side=700):
+def workload(name, side=700, batch=256):
     from pyglu import synth
 
     if name == "mesh":
@@ -71,8 +72,8 @@ def workload(name, side=700):
                     desc=f"largest system of the uneven batch, n={n}, {k} RHS, refine to 1e-10",
                     b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
     A = synth.config2_pattern()
-    return dict(A=A, batch=256, nrhs=4, tol=1e-10, values=1,
-                desc="256 value sets of one nodal pattern n=20000, 4 RHS each, refine to 1e-10",
+    return dict(A=A, batch=batch, nrhs=4, tol=1e-10, values=1,
+                desc=f"{batch} value sets of one nodal pattern n=20000, 4 RHS each, refine to 1e-10",
                 b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
 
 
@@ -299,7 +300,7 @@ def main():
         if pg:
             pg.destroy_process_group()
         return
-    W = workload(args.workload, args.side)
+    W = workload(args.workload, args.side, args.batch)
     if args.impl == "reference":
         if rank != 0:  # rank 0 alone times the reference; no collective follows
             if pg:
