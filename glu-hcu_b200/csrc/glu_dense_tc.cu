@@ -160,10 +160,14 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// x rounded to TF32 (1 + 10 explicit significand bits), ties away from zero,
+// as an FP32 value whose 13 low significand bits are zero: adding half a TF32
+// unit in the last place to the magnitude bits and clearing the 13 bits
+// below it (a carry into the exponent is the correct rounding up).  Done on
+// the bits so that every part of the split is exactly representable in TF32
+// whatever a conversion instruction leaves in the low bits; finite inputs.
 __device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 struct Tile {

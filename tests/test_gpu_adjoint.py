@@ -8,8 +8,10 @@ the small-matrix check in test_gpu_parity.
 * n = 20,000: FP64 central differences (relative step 1e-6) on 16 nonzeros
   and 16 entries of b, 1e-6 relative.  The function values come from the
   engine's FP64-refined solve (relative residual 1e-15 asked); the
-  differences are taken on entries whose relative sensitivity FP64 can
-  resolve (|v_q g_q| / |f| >= 1e-3), as in the small check.
+  differences are taken on the entries of largest relative sensitivity
+  |v_q g_q| / |f|: a central difference at relative step h resolves a
+  gradient to about (forward error of f) / (h * sensitivity), so only the
+  most sensitive entries of a system this size are resolved to 1e-6 by FP64.
 """
 import numpy as np
 import pytest
@@ -73,8 +75,8 @@ def test_adjoint_matches_central_differences_n20000():
     rng = np.random.default_rng(5)
     f0 = abs(loss)
     sens = np.abs(data * gv) / f0
-    cand = np.nonzero(sens >= 1e-3)[0]
-    assert cand.size >= 16
+    cand = np.argsort(sens)[-64:]  # the 64 most sensitive nonzeros
+    assert sens[cand].min() >= 1e-3
     for q in rng.choice(cand, 16, replace=False):
         h = 1e-6 * abs(data[q])
         vp, vm = data.copy(), data.copy()
@@ -84,8 +86,8 @@ def test_adjoint_matches_central_differences_n20000():
         assert abs(fd - gv[q]) <= 1e-6 * abs(fd), (q, fd, gv[q])
     lu.refactor(data)
     sb = np.abs(bn * gb) / f0
-    cand_b = np.nonzero(sb >= 1e-3)[0]
-    assert cand_b.size >= 16
+    cand_b = np.argsort(sb)[-64:]
+    assert sb[cand_b].min() >= 1e-3
     for i in rng.choice(cand_b, 16, replace=False):
         h = 1e-6 * abs(bn[i])
         bp, bm = bn.copy(), bn.copy()
