@@ -49,6 +49,7 @@ def parse():
                    help="skip the batched same-pattern sub-record of the mesh line")
     p.add_argument("--side", type=int, default=700, help="mesh side (workload mesh)")
     p.add_argument("--batch", type=int, default=256, help="value sets of the batch workload")
+    p.add_argument("--uneven-max-n", type=int, default=50000, help="largest system of the uneven workload")
     return p.parse_args()
 
 
@@ -66,7 +67,7 @@ def workload(name, side=700, batch=256):
                     desc="nodal matrix n=4960, 1 RHS, refine to 1e-10",
                     b=lambda n, k, s: synth.rhs_uniform(n, k, seed=s))
     if name == "uneven":  # the reference arm times one system of the set (its largest)
-        n, k, sd = max(synth.config3_systems(count=64, seed=0, n_range=(2000, 12000), rhs_range=(1, 64)))
+        n, k, sd = max(synth.config3_systems(count=64, seed=0, n_range=(2000, 50000), rhs_range=(1, 64)))
         A = synth.nodal(n, seed=sd)
         return dict(A=A, batch=1, nrhs=k, tol=1e-10, values=2,
                     desc=f"largest system of the uneven batch, n={n}, {k} RHS, refine to 1e-10",
@@ -201,20 +202,24 @@ def cpu_reference(W, steps, warmup, sample_only=False):
 
 
 def run_uneven(args, world, rank, local, pg):
-    """Uneven batch: 64 independent nodal systems of different sizes, each with
-    1-64 right-hand sides, refactored and FP64-refined together (UnevenBatch,
-    one stream per worker thread, host buffers)."""
+    """Uneven batch: 64 independent nodal systems of different sizes (n
+    log-uniform in [2,000, 50,000]), each with 1-64 right-hand sides,
+    refactored and FP64-refined together (UnevenBatch: every system's kernels
+    on one of 16 streams from one host thread, one host wait per
+    factorization round and per refinement step; host buffers)."""
     import torch
 
     import pyglu
     from pyglu import synth
 
     torch.cuda.set_device(local)
-    specs = synth.config3_systems(count=64, seed=0, n_range=(2000, 12000), rhs_range=(1, 64))
+    specs = synth.config3_systems(count=64, seed=0, n_range=(2000, args.uneven_max_n), rhs_range=(1, 64))
     systems = [synth.nodal(n, seed=sd) for n, k, sd in specs]
     bs = [synth.rhs_uniform(n, k, seed=sd).T.copy() for n, k, sd in specs]
     vals = [synth.perturb_values(*A, count=2, seed=7) for A in systems]
-    ub = pyglu.UnevenBatch(systems, workers=16, device=local)
+    t_setup = time.perf_counter()
+    ub = pyglu.UnevenBatch(systems, streams=16, workers=16, device=local)
+    t_setup = time.perf_counter() - t_setup
     solves = sum(k for _, k, _ in specs)
 
     def step(i):
@@ -241,10 +246,11 @@ def run_uneven(args, world, rank, local, pg):
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": nsteps,
             "warmup": nwarmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 nodal systems, n log-uniform in [2,000, 12,000] (the uneven-batch "
-                                   "shape at reduced sizes), 1-64 RHS each, refine to 1e-10",
+            "config": {"workload": f"64 nodal systems, n log-uniform in [2,000, {args.uneven_max_n:,}], "
+                                   "1-64 RHS each, refine to 1e-10",
                        "systems": len(specs), "rhs_total": solves, "n_total": sum(n for n, _, _ in specs),
-                       "parallelism": f"16 streams x{world}"},
+                       "nnz_lu_total": int(sum(lu.analysis.nnz_lu for lu in ub.lus)),
+                       "setup_s": t_setup, "parallelism": f"16 streams x{world}"},
             "residual": res, "refine_dtype": "f64",
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "note": "the uneven batch is driven through host buffers; value is already end to end"},

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "glu_internal.h"
@@ -229,6 +230,9 @@ struct glu_handle_s {
     uint32_t num_sms = 148;
     uint32_t spin_limit = kSpinLimit;
     bool inject_unset_flag = false;  // GLU_INJECT_UNSET_SOLVE_FLAG, for the next solve
+    // statistics of a factorization enqueued and not yet finished
+    uint64_t pending_launches = 0;
+    double pending_upd_bytes = 0, pending_upd_flops = 0;
     KernelProfiler prof;
     bool factored = false;
     glu_stats stats{};
@@ -1362,12 +1366,15 @@ glu_status glu_load_source_values(glu_handle_t h, uint32_t first, uint32_t count
     return GLU_OK;
 }
 
-glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int perturb, glu_stream stream) {
-    if (!h) return set_error(GLU_ERR_ARG, "null handle");
-    Status s = check_range(h, first, count);
-    if (s != GLU_OK) return s;
-    DeviceGuard g(h->device);
-    cudaStream_t st = S_(stream);
+}  // extern "C"
+
+namespace {
+
+// Everything of a factorization up to its last launch, on st; the status word
+// (and the perturbation of value set `first`) are copied to pinned memory
+// asynchronously.  factor_finish reads them once st has completed.
+Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int perturb, cudaStream_t st) {
+    Status s = GLU_OK;
     float *val = h->d_val.as<float>() + size_t(first) * h->nnz;
     const uint64_t stride = h->nnz;
     const float *pert = nullptr;
@@ -1550,21 +1557,82 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
     GLU_LAUNCH(KK_CHECK, launch_check_pivots(h->P, val, stride, count, h->d_status.as<uint32_t>(), st), "pivot check");
 #undef GLU_LAUNCH
     GLU_CUDA(cudaEventRecord(h->ev1, st), "event");
-    uint32_t flags = 0;
-    s = read_status(h, st, &flags);
-    if (s != GLU_OK) return s;
-    pf.collect();
+    GLU_CUDA(cudaMemcpyAsync(h->h_status, h->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+             "read status");
+    if (perturb)
+        GLU_CUDA(cudaMemcpyAsync(h->h_status + 1, h->d_pert.as<float>() + first, sizeof(float),
+                                 cudaMemcpyDeviceToHost, st),
+                 "read perturbation");
+    h->pending_launches = nlaunch;
+    h->pending_upd_bytes = upd_bytes;
+    h->pending_upd_flops = upd_flops;
+    return s;
+}
+
+// The host half of a factorization whose stream has completed: status,
+// statistics, per-kernel times.
+Status factor_finish(glu_handle_s *h, int perturb) {
+    const uint32_t flags = h->h_status[0];
+    h->prof.collect();
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.last_factor_ms = ms;
-    h->stats.factor_launches = nlaunch;
-    h->stats.dense_update_bytes = upd_bytes;
-    h->stats.dense_update_flops = upd_flops;
-    if (perturb) cudaMemcpy(&h->stats.pert, h->d_pert.as<float>() + first, sizeof(float), cudaMemcpyDeviceToHost);
+    h->stats.factor_launches = h->pending_launches;
+    h->stats.dense_update_bytes = h->pending_upd_bytes;
+    h->stats.dense_update_flops = h->pending_upd_flops;
+    if (perturb) std::memcpy(&h->stats.pert, h->h_status + 1, sizeof(float));
     h->factored = true;
     if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "factorization wait timed out");
     if (flags & (DEV_ZERO_PIVOT | DEV_NONFINITE_PIVOT))
         return set_error(GLU_ERR_SINGULAR, "%s pivot encountered", (flags & DEV_ZERO_PIVOT) ? "zero" : "non-finite");
+    return GLU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int perturb, glu_stream stream) {
+    if (!h) return set_error(GLU_ERR_ARG, "null handle");
+    Status s = check_range(h, first, count);
+    if (s != GLU_OK) return s;
+    DeviceGuard g(h->device);
+    cudaStream_t st = S_(stream);
+    s = factor_enqueue(h, first, count, perturb, st);
+    if (s != GLU_OK) return s;
+    GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
+    return factor_finish(h, perturb);
+}
+
+glu_status glu_factor_many(uint32_t count, const glu_handle_t *handles, int perturb, const glu_stream *streams,
+                           uint32_t nstreams) {
+    if (count == 0) return GLU_OK;
+    if (!handles || (nstreams && !streams)) return set_error(GLU_ERR_ARG, "null argument");
+    for (uint32_t i = 0; i < count; ++i)
+        if (!handles[i]) return set_error(GLU_ERR_ARG, "null handle %u", i);
+    auto stream_of = [&](uint32_t i) { return nstreams ? S_(streams[i % nstreams]) : cudaStream_t(nullptr); };
+    // every system's launches first, each on its stream ...
+    for (uint32_t i = 0; i < count; ++i) {
+        glu_handle_s *h = handles[i];
+        DeviceGuard g(h->device);
+        Status s = factor_enqueue(h, 0, h->batch, perturb, stream_of(i));
+        if (s != GLU_OK) return set_error(s, "system %u: %s", i, glu_last_error());
+    }
+    // ... then one wait per stream, then every system's status
+    for (uint32_t i = 0; i < std::max<uint32_t>(nstreams, 1) && i < count; ++i) {
+        DeviceGuard g(handles[i]->device);
+        GLU_CUDA(cudaStreamSynchronize(stream_of(i)), "synchronize");
+    }
+    Status first_err = GLU_OK;
+    std::string msg;
+    for (uint32_t i = 0; i < count; ++i) {
+        Status s = factor_finish(handles[i], perturb);
+        if (s != GLU_OK && first_err == GLU_OK) {
+            first_err = s;
+            msg = "system " + std::to_string(i) + ": " + glu_last_error();
+        }
+    }
+    if (first_err != GLU_OK) return set_error(first_err, "%s", msg.c_str());
     return GLU_OK;
 }
 
@@ -1580,100 +1648,239 @@ glu_status glu_solve_transposed(glu_handle_t h, uint32_t inst, uint32_t nrhs, co
     return solve_f32(h, inst, nrhs, b, x, where, true, S_(stream));
 }
 
+}  // extern "C"
+
+namespace {
+
+// A refined solve of value sets [first, first + count) of one handle, run as
+// a sequence of enqueued steps so that many of them (glu_solve_refined_many)
+// can advance together with one host synchronisation per step.
+struct RefineJob {
+    glu_handle_s *h = nullptr;
+    uint32_t first = 0, count = 0, nrhs = 0;
+    const double *b = nullptr;
+    double *x = nullptr;
+    double tol = 0;
+    uint32_t maxit = 0;
+    bool tr = false, host = false;
+    cudaStream_t st = nullptr;
+    // state
+    uint32_t nvec = 0, it = 0;
+    size_t len = 0;
+    const double *bz = nullptr;
+    double *xz = nullptr;
+    double worst2 = 0, worstinf = 0;
+    bool done = false;
+};
+
+Status refine_prepare(RefineJob &j) {
+    glu_handle_s *h = j.h;
+    if (!h->factored) return set_error(GLU_ERR_STATE, "solve before factorization");
+    if (!h->has_source || !h->ax0_loaded)
+        return set_error(GLU_ERR_STATE, "refinement needs the source matrix values (glu_load_source_values)");
+    if (uint64_t(j.nrhs) * j.count > 65535)
+        return set_error(GLU_ERR_UNSUPPORTED, "count * nrhs = %llu right-hand sides exceed 65,535 per call",
+                         (unsigned long long)j.nrhs * j.count);
+    j.nvec = j.nrhs * j.count;
+    j.len = size_t(h->n) * j.nvec;
+    GLU_CUDA(h->d_y.ensure(sizeof(float) * j.len), "allocate");
+    GLU_CUDA(h->d_b64.ensure(sizeof(double) * j.len * (j.host ? 1 : 0) + 8), "allocate");
+    GLU_CUDA(h->d_x64.ensure(sizeof(double) * j.len * (j.host ? 1 : 0) + 8), "allocate");
+    GLU_CUDA(h->d_r64.ensure(sizeof(double) * j.len), "allocate");
+    GLU_CUDA(h->d_norms.ensure(sizeof(double) * 4 * j.nvec), "allocate");
+    if (h->h_norms_cap < 4 * size_t(j.nvec)) {
+        if (h->h_norms) cudaFreeHost(h->h_norms);
+        h->h_norms = nullptr;
+        h->h_norms_cap = 0;
+        GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_norms), sizeof(double) * 4 * j.nvec),
+                 "allocate pinned");
+        h->h_norms_cap = 4 * size_t(j.nvec);
+    }
+    return GLU_OK;
+}
+
+// r = b - A0 x for every vector, norms to the host (asynchronously).
+Status refine_residual(RefineJob &j) {
+    glu_handle_s *h = j.h;
+    const uint32_t *rptr = j.tr ? h->d_a0_cptr.as<uint32_t>() : h->d_a0_rptr.as<uint32_t>();
+    const uint32_t *cidx = j.tr ? h->d_a0_ridx.as<uint32_t>() : h->d_a0_cidx.as<uint32_t>();
+    const uint32_t *vmap = j.tr ? h->d_a0_ident.as<uint32_t>() : h->d_a0_vmap.as<uint32_t>();
+    const double *ax0 = h->d_ax0.as<double>() + size_t(j.first) * h->nnz_src;
+    double *norms = h->d_norms.as<double>();
+    GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, h->n, j.bz, j.xz, h->d_r64.as<double>(), j.nvec, j.nrhs,
+                             h->nnz_src, norms, j.st),
+             "residual");
+    GLU_CUDA(cudaMemcpyAsync(h->h_norms, norms, sizeof(double) * 4 * j.nvec, cudaMemcpyDeviceToHost, j.st),
+             "read norms");
+    return GLU_OK;
+}
+
+// x = solve(v) (accumulate: x += solve(v)) for every vector v of src.
+Status refine_solve(RefineJob &j, const double *src, int accumulate) {
+    glu_handle_s *h = j.h;
+    const TransformDev &T = h->T;
+    float *y = h->d_y.as<float>();
+    GLU_CUDA(launch_transform_f64_to_f32(j.tr ? T.tin_idx : T.in_idx, j.tr ? T.tin_scale : T.in_scale, src, y, h->n,
+                                         j.nvec, j.st),
+             "transform");
+    Status s = solve_inplace(h, j.first, j.count, y, j.nrhs, j.tr, j.st);
+    if (s != GLU_OK) return s;
+    GLU_CUDA(launch_transform_f32_to_f64_add(j.tr ? T.tout_idx : T.out_idx, j.tr ? T.tout_scale : T.out_scale, y,
+                                             j.xz, h->n, j.nvec, accumulate, j.st),
+             "transform");
+    return GLU_OK;
+}
+
+// Enqueues x0 = solve(b) and the first residual.
+Status refine_start(RefineJob &j) {
+    glu_handle_s *h = j.h;
+    if (j.host) {
+        GLU_CUDA(cudaMemcpyAsync(h->d_b64.p, j.b, sizeof(double) * j.len, cudaMemcpyHostToDevice, j.st), "copy b");
+        j.bz = h->d_b64.as<double>();
+        j.xz = h->d_x64.as<double>();
+    } else {
+        j.bz = j.b;
+        j.xz = j.x;
+    }
+    double *norms = h->d_norms.as<double>();
+    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), j.st), "reset status");
+    GLU_CUDA(launch_norms(j.bz, h->n, j.nvec, norms + 2 * j.nvec, j.st), "norms");
+    Status s = refine_solve(j, j.bz, 0);
+    if (s != GLU_OK) return s;
+    return refine_residual(j);
+}
+
+// After the stream has completed the last residual: stop, or enqueue
+// x += solve(r) and the next residual.
+Status refine_step(RefineJob &j) {
+    glu_handle_s *h = j.h;
+    const double *hn = h->h_norms;
+    j.worst2 = 0;
+    j.worstinf = 0;
+    for (uint32_t v = 0; v < j.nvec; ++v) {
+        double bn2 = std::sqrt(hn[2 * j.nvec + 2 * v]), bninf = hn[2 * j.nvec + 2 * v + 1];
+        double rn2 = std::sqrt(hn[2 * v]), rninf = hn[2 * v + 1];
+        double rel2 = bn2 > 0 ? rn2 / bn2 : rn2, relinf = bninf > 0 ? rninf / bninf : rninf;
+        if (!(rel2 == rel2)) rel2 = INFINITY;
+        j.worst2 = std::max(j.worst2, rel2);
+        j.worstinf = std::max(j.worstinf, relinf);
+    }
+    if (j.worst2 <= j.tol || j.it >= j.maxit) {
+        j.done = true;
+        if (j.host)
+            GLU_CUDA(cudaMemcpyAsync(j.x, j.xz, sizeof(double) * j.len, cudaMemcpyDeviceToHost, j.st), "copy x");
+        GLU_CUDA(cudaMemcpyAsync(h->h_status, h->d_status.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, j.st),
+                 "read status");
+        return GLU_OK;
+    }
+    ++j.it;
+    Status s = refine_solve(j, h->d_r64.as<double>(), 1);
+    if (s != GLU_OK) return s;
+    return refine_residual(j);
+}
+
+// After the stream has completed the job's last step.
+Status refine_finish(RefineJob &j, glu_refine_stats *stats) {
+    if (j.h->h_status[0] & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
+    if (stats) *stats = glu_refine_stats{j.it, j.worst2, j.worstinf};
+    if (!(j.worst2 <= j.tol))
+        return set_error(GLU_ERR_NOT_CONVERGED, "refinement stopped at relative residual %.3e > %.3e", j.worst2,
+                         j.tol);
+    return GLU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uint32_t nrhs,
                              const double *b, double *x, double tol, uint32_t maxit, int transposed,
                              glu_memory where, glu_refine_stats *stats, glu_stream stream) {
     if (!h || !b || !x) return set_error(GLU_ERR_ARG, "null argument");
     Status s = check_range(h, first, count);
     if (s != GLU_OK) return s;
-    if (!h->factored) return set_error(GLU_ERR_STATE, "solve before factorization");
-    if (!h->has_source || !h->ax0_loaded)
-        return set_error(GLU_ERR_STATE, "refinement needs the source matrix values (glu_load_source_values)");
     if (nrhs == 0) return GLU_OK;
-    if (uint64_t(nrhs) * count > 65535)
-        return set_error(GLU_ERR_UNSUPPORTED, "count * nrhs = %llu right-hand sides exceed 65,535 per call",
-                         (unsigned long long)nrhs * count);
     DeviceGuard g(h->device);
-    cudaStream_t st = S_(stream);
-    const uint32_t n = h->n;
-    // every value set's right-hand sides together: nvec vectors of n
-    const uint32_t nvec = nrhs * count;
-    const size_t len = size_t(n) * nvec;
-    GLU_CUDA(h->d_y.ensure(sizeof(float) * len), "allocate");
-    GLU_CUDA(h->d_b64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
-    GLU_CUDA(h->d_x64.ensure(sizeof(double) * len * (where == GLU_HOST ? 1 : 0) + 8), "allocate");
-    GLU_CUDA(h->d_r64.ensure(sizeof(double) * len), "allocate");
-    GLU_CUDA(h->d_norms.ensure(sizeof(double) * 4 * nvec), "allocate");
-    if (h->h_norms_cap < 4 * size_t(nvec)) {
-        if (h->h_norms) cudaFreeHost(h->h_norms);
-        h->h_norms = nullptr;
-        GLU_CUDA(cudaMallocHost(reinterpret_cast<void **>(&h->h_norms), sizeof(double) * 4 * nvec), "allocate pinned");
-        h->h_norms_cap = 4 * size_t(nvec);
+    RefineJob j;
+    j.h = h;
+    j.first = first;
+    j.count = count;
+    j.nrhs = nrhs;
+    j.b = b;
+    j.x = x;
+    j.tol = tol;
+    j.maxit = maxit;
+    j.tr = transposed != 0;
+    j.host = where == GLU_HOST;
+    j.st = S_(stream);
+    if ((s = refine_prepare(j)) != GLU_OK || (s = refine_start(j)) != GLU_OK) return s;
+    // every value set in each step, until the worst relative residual of all
+    // right-hand sides meets tol (one synchronisation per step)
+    while (!j.done) {
+        GLU_CUDA(cudaStreamSynchronize(j.st), "synchronize");
+        if ((s = refine_step(j)) != GLU_OK) return s;
     }
-    const TransformDev &T = h->T;
-    const bool tr = transposed != 0;
-    const uint32_t *in_idx = tr ? T.tin_idx : T.in_idx;
-    const double *in_s = tr ? T.tin_scale : T.in_scale;
-    const uint32_t *out_idx = tr ? T.tout_idx : T.out_idx;
-    const double *out_s = tr ? T.tout_scale : T.out_scale;
-    const uint32_t *rptr = tr ? h->d_a0_cptr.as<uint32_t>() : h->d_a0_rptr.as<uint32_t>();
-    const uint32_t *cidx = tr ? h->d_a0_ridx.as<uint32_t>() : h->d_a0_cidx.as<uint32_t>();
-    const uint32_t *vmap = tr ? h->d_a0_ident.as<uint32_t>() : h->d_a0_vmap.as<uint32_t>();
-    float *y = h->d_y.as<float>();
-    double *r = h->d_r64.as<double>();
-    double *norms = h->d_norms.as<double>();
-    const double *bz;
-    double *xz;
-    if (where == GLU_HOST) {
-        GLU_CUDA(cudaMemcpyAsync(h->d_b64.p, b, sizeof(double) * len, cudaMemcpyHostToDevice, st), "copy b");
-        bz = h->d_b64.as<double>();
-        xz = h->d_x64.as<double>();
-    } else {
-        bz = b;
-        xz = x;
+    GLU_CUDA(cudaStreamSynchronize(j.st), "synchronize");
+    return refine_finish(j, stats);
+}
+
+glu_status glu_solve_refined_many(uint32_t count, const glu_handle_t *handles, const uint32_t *nrhs,
+                                  const double *const *b, double *const *x, double tol, uint32_t maxit,
+                                  glu_memory where, glu_refine_stats *stats, const glu_stream *streams,
+                                  uint32_t nstreams) {
+    if (count == 0) return GLU_OK;
+    if (!handles || !nrhs || !b || !x || (nstreams && !streams)) return set_error(GLU_ERR_ARG, "null argument");
+    std::vector<RefineJob> jobs(count);
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!handles[i] || !b[i] || !x[i]) return set_error(GLU_ERR_ARG, "null argument of system %u", i);
+        RefineJob &j = jobs[i];
+        j.h = handles[i];
+        j.first = 0;
+        j.count = j.h->batch;
+        j.nrhs = nrhs[i];
+        j.b = b[i];
+        j.x = x[i];
+        j.tol = tol;
+        j.maxit = maxit;
+        j.host = where == GLU_HOST;
+        j.st = nstreams ? S_(streams[i % nstreams]) : nullptr;
+        j.done = j.nrhs == 0;
     }
-    const double *ax0 = h->d_ax0.as<double>() + size_t(first) * h->nnz_src;
-    GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
-    GLU_CUDA(launch_norms(bz, n, nvec, norms + 2 * nvec, st), "norms");
-    // x0 = solve(b), every value set at once
-    GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, bz, y, n, nvec, st), "transform");
-    s = solve_inplace(h, first, count, y, nrhs, tr, st);
-    if (s != GLU_OK) return s;
-    GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nvec, 0, st), "transform");
-    // r = b - A0 x, x += solve(r), with every value set in each step, until the
-    // worst relative residual of all right-hand sides meets tol
-    uint32_t it = 0;
-    double worst2 = 0, worstinf = 0;
-    for (;; ++it) {
-        GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, n, bz, xz, r, nvec, nrhs, h->nnz_src, norms, st), "residual");
-        GLU_CUDA(cudaMemcpyAsync(h->h_norms, norms, sizeof(double) * 4 * nvec, cudaMemcpyDeviceToHost, st),
-                 "read norms");
-        GLU_CUDA(cudaStreamSynchronize(st), "synchronize");
-        worst2 = 0;
-        worstinf = 0;
-        for (uint32_t v = 0; v < nvec; ++v) {
-            double bn2 = std::sqrt(h->h_norms[2 * nvec + 2 * v]), bninf = h->h_norms[2 * nvec + 2 * v + 1];
-            double rn2 = std::sqrt(h->h_norms[2 * v]), rninf = h->h_norms[2 * v + 1];
-            double rel2 = bn2 > 0 ? rn2 / bn2 : rn2, relinf = bninf > 0 ? rninf / bninf : rninf;
-            if (!(rel2 == rel2)) rel2 = INFINITY;
-            worst2 = std::max(worst2, rel2);
-            worstinf = std::max(worstinf, relinf);
+    auto fail = [&](uint32_t i, Status s) { return set_error(s, "system %u: %s", i, glu_last_error()); };
+    for (uint32_t i = 0; i < count; ++i) {
+        if (jobs[i].done) continue;
+        DeviceGuard g(jobs[i].h->device);
+        Status s = refine_prepare(jobs[i]);
+        if (s == GLU_OK) s = refine_start(jobs[i]);
+        if (s != GLU_OK) return fail(i, s);
+    }
+    const uint32_t nsync = std::max<uint32_t>(std::min(nstreams, count), 1);
+    for (;;) {
+        bool pending = false;
+        for (uint32_t i = 0; i < count; ++i) pending |= !jobs[i].done;
+        for (uint32_t k = 0; k < nsync; ++k) {
+            DeviceGuard g(jobs[k].h->device);
+            GLU_CUDA(cudaStreamSynchronize(jobs[k].st), "synchronize");
         }
-        if (worst2 <= tol || it >= maxit) break;
-        GLU_CUDA(launch_transform_f64_to_f32(in_idx, in_s, r, y, n, nvec, st), "transform");
-        s = solve_inplace(h, first, count, y, nrhs, tr, st);
-        if (s != GLU_OK) return s;
-        GLU_CUDA(launch_transform_f32_to_f64_add(out_idx, out_s, y, xz, n, nvec, 1, st), "transform");
+        if (!pending) break;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (jobs[i].done) continue;
+            DeviceGuard g(jobs[i].h->device);
+            Status s = refine_step(jobs[i]);
+            if (s != GLU_OK) return fail(i, s);
+        }
     }
-    if (where == GLU_HOST)
-        GLU_CUDA(cudaMemcpyAsync(x, xz, sizeof(double) * len, cudaMemcpyDeviceToHost, st), "copy x");
-    uint32_t flags = 0;
-    s = read_status(h, st, &flags);
-    if (s != GLU_OK) return s;
-    if (flags & DEV_TIMEOUT) return set_error(GLU_ERR_TIMEOUT, "solve dependency wait timed out");
-    if (stats) *stats = glu_refine_stats{it, worst2, worstinf};
-    if (!(worst2 <= tol))
-        return set_error(GLU_ERR_NOT_CONVERGED, "refinement stopped at relative residual %.3e > %.3e", worst2, tol);
+    Status first_err = GLU_OK;
+    std::string msg;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (jobs[i].nrhs == 0) continue;
+        Status s = refine_finish(jobs[i], stats ? stats + i : nullptr);
+        if (s != GLU_OK && first_err == GLU_OK) {
+            first_err = s;
+            msg = "system " + std::to_string(i) + ": " + glu_last_error();
+        }
+    }
+    if (first_err != GLU_OK) return set_error(first_err, "%s", msg.c_str());
     return GLU_OK;
 }
 

@@ -227,10 +227,20 @@ class GLUFactorization:
     """
 
     def __init__(self, data, indices, indptr, n, perturb=False, device=0):
-        self._an = Analysis(data, indices, indptr, n)
+        self._setup(Analysis(data, indices, indptr, n), perturb, device)
+
+    def _setup(self, an, perturb, device):
+        self._an = an
         self._eng = _Engine(self._an, 1, device)
         self.perturb = bool(perturb)
         self._factor_values(self._an.data)
+
+    @classmethod
+    def _from_analysis(cls, an, perturb=False, device=0):
+        """A factorization of an already analysed matrix."""
+        obj = cls.__new__(cls)
+        obj._setup(an, perturb, device)
+        return obj
 
     # -- reference surface -------------------------------------------------
     @property
@@ -439,19 +449,28 @@ class UnevenBatch:
     """Independent systems of different sizes and patterns, each with its own
     right-hand sides, refactored and solved together.
 
-    ``systems`` is a list of CSC matrices ``(data, indices, indptr, n)``.  Every
-    system keeps its own analysis, handle and CUDA stream; ``workers`` host
-    threads drive them, so the launches of different systems overlap on the
-    GPU (the engine's calls release the GIL).  The same FP32 factorization and
-    FP64 refinement as ``GLUFactorization`` apply to each system; ``refactor``
-    keeps each system's ordering and scaling, as a refactorization does.
+    ``systems`` is a list of CSC matrices ``(data, indices, indptr, n)``.  Each
+    system keeps its own analysis and handle; refactorization and refined
+    solves go through glu_factor_many / glu_solve_refined_many: every system's
+    kernels are enqueued on one of ``streams`` CUDA streams from one host
+    thread, and the host waits once per factorization round and once per
+    refinement step for all systems together.  The analyses (NICSLU
+    preprocessing and the symbolic phase, on the host) run in ``workers``
+    threads.  ``refactor`` keeps each system's ordering and scaling, as a
+    refactorization does.
     """
 
-    def __init__(self, systems, perturb=False, device=0, workers=8):
+    def __init__(self, systems, perturb=False, device=0, streams=16, workers=8):
+        import concurrent.futures as cf
+
         torch = _torch()
-        self.lus = [GLUFactorization(*sys_, perturb=perturb, device=device) for sys_ in systems]
-        self.workers = max(1, min(int(workers), len(self.lus)))
-        self._streams = [torch.cuda.Stream(device=device) for _ in range(self.workers)]
+        systems = list(systems)
+        with cf.ThreadPoolExecutor(max(1, min(int(workers), len(systems)))) as ex:
+            analyses = list(ex.map(lambda s_: Analysis(*s_), systems))
+        self.lus = [GLUFactorization._from_analysis(an, perturb=perturb, device=device) for an in analyses]
+        self._streams = [torch.cuda.Stream(device=device) for _ in range(max(1, min(int(streams), len(self.lus))))]
+        self._stream_ptrs = (_capi.C.c_void_p * len(self._streams))(*[s_.cuda_stream for s_ in self._streams])
+        self._handles = (_capi.C.c_void_p * len(self.lus))(*[lu.handle.value for lu in self.lus])
         self.perturb = bool(perturb)
         self.last_refine = None
 
@@ -466,20 +485,6 @@ class UnevenBatch:
         """FP32 factor values of system i (Symbolic_Matrix::val layout)."""
         return self.lus[i].lu_values()
 
-    def _run(self, fn):
-        import concurrent.futures as cf
-
-        with cf.ThreadPoolExecutor(self.workers) as ex:
-            futs = [ex.submit(self._worker, w, fn) for w in range(self.workers)]
-            out = {}
-            for f in futs:
-                out.update(f.result())
-        return [out[i] for i in range(len(self.lus))]
-
-    def _worker(self, w, fn):
-        st = _capi.C.c_void_p(self._streams[w].cuda_stream)
-        return {i: fn(i, st) for i in range(w, len(self.lus), self.workers)}
-
     def refactor(self, values):
         """New values for every system (a list of data arrays, CSC order)."""
         eng = _capi.engine()
@@ -489,14 +494,12 @@ class UnevenBatch:
         for v, lu in zip(vals, self.lus):
             if v.shape != (lu._an.nnz_a,):
                 raise ValueError(f"expected {lu._an.nnz_a} values, got shape {v.shape}")
-
-        def fn(i, st):
-            lu = self.lus[i]
-            check(eng.glu_load_source_values(lu._eng._h, 0, 1, ptr(vals[i]), _capi.GLU_HOST, st), "value upload")
-            check(eng.glu_factor(lu._eng._h, 0, 1, 1 if self.perturb else 0, st), "GPU factorization")
-            return None
-
-        self._run(fn)
+        ns = len(self._streams)
+        for i, (v, lu) in enumerate(zip(vals, self.lus)):
+            check(eng.glu_load_source_values(lu._eng._h, 0, 1, ptr(v), _capi.GLU_HOST,
+                                             _capi.C.c_void_p(self._stream_ptrs[i % ns])), "value upload")
+        check(eng.glu_factor_many(len(self.lus), self._handles, 1 if self.perturb else 0, self._stream_ptrs, ns),
+              "GPU factorization")
         return self
 
     def solve(self, bs, tol=1e-10, maxiter=10):
@@ -505,30 +508,31 @@ class UnevenBatch:
         eng = _capi.engine()
         if len(bs) != len(self.lus):
             raise ValueError(f"expected {len(self.lus)} right-hand sides, got {len(bs)}")
-        mats = []
+        vecs, mats, xs = [], [], []
         for b, lu in zip(bs, self.lus):
             b = np.asarray(b, dtype=np.float64)
             if b.shape[0] != lu.n:
                 raise ValueError(f"RHS length {b.shape[0]} != matrix dimension {lu.n}")
-            mats.append((b.ndim == 1, np.ascontiguousarray(b.reshape(lu.n, -1).T)))
-        stats = [None] * len(self.lus)
-
-        def fn(i, st):
-            lu = self.lus[i]
-            vec, bm = mats[i]
-            x = np.empty_like(bm)
-            rs = _capi.RefineStats()
-            s = eng.glu_solve_refined(lu._eng._h, 0, 1, bm.shape[0], ptr(bm), ptr(x), float(tol), int(maxiter), 0,
-                                      _capi.GLU_HOST, _capi.C.byref(rs), st)
-            if s != _capi.GLU_ERR_NOT_CONVERGED:
-                check(s, "refined solve")
-            stats[i] = dict(iterations=rs.iterations, residual=rs.residual, residual_inf=rs.residual_inf)
+            bm = np.ascontiguousarray(b.reshape(lu.n, -1).T)  # (k, n)
+            vecs.append(b.ndim == 1)
+            mats.append(bm)
+            xs.append(np.empty_like(bm))
+        count = len(self.lus)
+        nrhs = (_capi.C.c_uint32 * count)(*[m.shape[0] for m in mats])
+        bp = (_capi.C.c_void_p * count)(*[m.ctypes.data for m in mats])
+        xp = (_capi.C.c_void_p * count)(*[x.ctypes.data for x in xs])
+        stats = (_capi.RefineStats * count)()
+        s = eng.glu_solve_refined_many(count, self._handles, nrhs, bp, xp, float(tol), int(maxiter), _capi.GLU_HOST,
+                                       stats, self._stream_ptrs, len(self._streams))
+        if s != _capi.GLU_ERR_NOT_CONVERGED:
+            check(s, "refined solve")
+        self.last_refine = [dict(iterations=st.iterations, residual=st.residual, residual_inf=st.residual_inf)
+                            for st in stats]
+        out = []
+        for vec, x in zip(vecs, xs):
             x = x.T
-            return np.ascontiguousarray(x[:, 0] if vec else x)
-
-        xs = self._run(fn)
-        self.last_refine = stats
-        return xs
+            out.append(np.ascontiguousarray(x[:, 0] if vec else x))
+        return out
 
 
 def write_mtx(path, data, indices, indptr, n):

@@ -39,6 +39,7 @@ ENGINE_SYMBOLS = [
     "glu_factor", "glu_solve", "glu_solve_transposed", "glu_solve_refined", "glu_get_stats",
     "glu_get_tuning", "glu_set_tuning", "glu_solve_noalloc", "glu_profile_enable", "glu_kernel_times",
     "glu_kernel_kind_name", "glu_measure_fp32_peak", "glu_set_wait_limit", "glu_debug_inject",
+    "glu_factor_many", "glu_solve_refined_many",
 ]
 GLU_KERNEL_KINDS = 15
 PRE_SYMBOLS = [
@@ -128,6 +129,9 @@ def load_engine():
         "glu_measure_fp32_peak": [C.c_int, C.POINTER(C.c_double)],
         "glu_set_wait_limit": [_vp, _u32],
         "glu_debug_inject": [_vp, C.c_int, _u32],
+        "glu_factor_many": [_u32, _vp, C.c_int, _vp, _u32],
+        "glu_solve_refined_many": [_u32, _vp, _vp, _vp, _vp, C.c_double, _u32, C.c_int,
+                                   C.POINTER(RefineStats), _vp, _u32],
     }
     for name, args in sig.items():
         f = getattr(lib, name)

@@ -185,6 +185,25 @@ glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uin
                              int transposed, glu_memory where, glu_refine_stats *stats,
                              glu_stream stream);
 
+/* -------------------------------------------------- many systems at once --
+ * Independent systems of different patterns and sizes (one handle each),
+ * factored or solved together: every system's kernels go to streams[i %
+ * nstreams] (nstreams 0: the legacy default stream) and the host waits once
+ * per call (factorization) or once per refinement step (solve) for all of
+ * them, instead of once per system.  No counterpart in the reference.
+ * glu_factor_many factors every value set of each handle.
+ * glu_solve_refined_many: system i solves its nrhs[i] right-hand sides per
+ * value set, b[i] / x[i] laid out as in glu_solve_refined; refinement steps of
+ * all systems run in lockstep, a system stops when its own residual meets
+ * tol.  stats (nullable) receives one record per system.  The first failing
+ * system's status is returned, its index in the message. */
+glu_status glu_factor_many(uint32_t count, const glu_handle_t *handles, int perturb, const glu_stream *streams,
+                           uint32_t nstreams);
+glu_status glu_solve_refined_many(uint32_t count, const glu_handle_t *handles, const uint32_t *nrhs,
+                                  const double *const *b, double *const *x, double tol, uint32_t maxit,
+                                  glu_memory where, glu_refine_stats *stats, const glu_stream *streams,
+                                  uint32_t nstreams);
+
 /* ------------------------------------------------------------------- stats --*/
 typedef struct {
     uint32_t n;
