@@ -1466,14 +1466,22 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     }
     uint32_t *dstatus = h->d_status.as<uint32_t>();
     double upd_bytes = 0, upd_flops = 0;
+    // A region goes to the tensor cores when it gives every SM at least two
+    // 128 x 128 tiles (over all value sets); thinner ones (the look-ahead
+    // strips, the last small updates) stay on the FP32 FMA kernel, whose
+    // launch costs less than the tensor-core kernel's set-up.
+    auto tc_region = [&](uint32_t rows, uint32_t cols) {
+        return tc && uint64_t(rows) * cols * count >= uint64_t(2) * h->num_sms * kTcTile * kTcTile;
+    };
     auto update = [&](uint32_t k0, uint32_t kb, DenseRegion reg, cudaStream_t s) -> cudaError_t {
-        const double rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
-        const double cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
+        const uint32_t nr = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
+        const uint32_t nc = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
+        const double rows = nr, cols = nc;
         upd_bytes += double(count) * (8.0 * rows * cols + 4.0 * kb * (rows + cols));
         upd_flops += double(count) * 2.0 * kb * rows * cols;
         cudaError_t e = pf.begin(s);
         if (e != cudaSuccess) return e;
-        if (tc) {
+        if (tc_region(nr, nc)) {
             e = launch_dense_update_tc(h->map_packA, h->map_packB, dbase, dstride, count, doff, h->m, k0, kb, dscr,
                                        reg, dstatus, h->spin_limit, h->num_sms, s);
             if (e == cudaSuccess) e = pf.end(KK_UPDATE_TC, s);
@@ -1486,8 +1494,8 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     };
     // TF32 hi/lo operands of panel k0 (slot0 0: first of a pair or alone; 64:
     // second of a pair), on the panel stream
-    auto pack = [&](uint32_t k0, uint32_t kb, uint32_t slot0) -> cudaError_t {
-        if (!tc) return cudaSuccess;
+    auto pack = [&](uint32_t k0, uint32_t kb, uint32_t slot0, bool needed) -> cudaError_t {
+        if (!needed) return cudaSuccess;
         cudaError_t e = pf.begin(ps);
         if (e == cudaSuccess)
             e = launch_dense_pack(dbase, dstride, count, doff, h->m, k0, kb, slot0, h->d_packA.as<float>(),
@@ -1511,9 +1519,21 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
             GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
             rest_pending = false;
         }
+        const bool single = rest0 <= nb || !lookahead;
+        // packs are written when any update of this step reads them: the
+        // single update, or one of the pair's strips and rest
+        bool packed = false;
+        if (single) {
+            packed = tc_region(rest0, rest0);
+        } else {
+            const uint32_t q1 = k0 + nb, qb1 = std::min<uint32_t>(nb, h->m - q1), r1 = h->m - (q1 + qb1);
+            packed = tc_region(nb, rest0) || tc_region(rest0 - nb, nb) ||
+                     (r1 <= nb ? tc_region(r1, r1)
+                               : (tc_region(nb, r1) || tc_region(r1 - nb, nb) || tc_region(r1 - nb, r1 - nb)));
+        }
         // after the previous pair's update, which reads the packs
-        GLU_CUDA(pack(k0, kb0, 0), "factor (dense pack)");
-        if (rest0 <= nb || !lookahead) {  // small trailing blocks, last panels: plain steps
+        GLU_CUDA(pack(k0, kb0, 0, packed), "factor (dense pack)");
+        if (single) {  // small trailing blocks, last panels: plain steps
             GLU_CUDA(update(k0, kb0, DenseRegion{0, rest0, 0, rest0, 1, k0}, ps), "factor (dense update)");
             k0 += kb0;
             continue;
@@ -1523,7 +1543,7 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         GLU_CUDA(update(k0, kb0, DenseRegion{0, nb, 0, rest0, 1, k0}, ps), "factor (dense update)");
         GLU_CUDA(update(k0, kb0, DenseRegion{nb, rest0, 0, nb, 0, k0}, ps), "factor (dense update)");
         GLU_CUDA(panel(k1, kb1), "factor (dense panel)");
-        GLU_CUDA(pack(k1, kb1, kDenseNB), "factor (dense pack)");
+        GLU_CUDA(pack(k1, kb1, kDenseNB, packed), "factor (dense pack)");
         const uint32_t rest1 = h->m - (k1 + kb1), kk = kb0 + kb1;
         if (rest1 <= nb) {
             GLU_CUDA(update(k0, kk, DenseRegion{0, rest1, 0, rest1, 1, k1}, ps), "factor (dense update)");

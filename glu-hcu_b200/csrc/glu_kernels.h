@@ -105,6 +105,7 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
 // computed by tcgen05 from TMA loads of the packs.  dense_tc_tensor_map
 // describes a pack buffer of `batch` value sets for the loads.
 constexpr uint32_t kDensePackRow = 384;
+constexpr uint32_t kTcTile = 128;  // update tile of the tensor-core kernel (M = N)
 cudaError_t dense_tc_tensor_map(float *pack, uint32_t m, uint32_t batch, CUtensorMap *map);
 cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count, const uint32_t *doff, uint32_t m,
                               uint32_t k0, uint32_t kb, uint32_t slot0, float *packA, float *packB,
