@@ -1466,13 +1466,14 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     }
     uint32_t *dstatus = h->d_status.as<uint32_t>();
     double upd_bytes = 0, upd_flops = 0;
-    // A region goes to the tensor cores when it gives every SM at least two
-    // 128 x 128 tiles (over all value sets); thinner ones (the look-ahead
-    // strips, the last small updates) stay on the FP32 FMA kernel, whose
-    // launch costs less than the tensor-core kernel's set-up.
-    auto tc_region = [&](uint32_t rows, uint32_t cols) {
-        return tc && uint64_t(rows) * cols * count >= uint64_t(2) * h->num_sms * kTcTile * kTcTile;
-    };
+    // A region goes to the tensor cores when its area over all value sets
+    // reaches two 128 x 128 tiles per SM, or dense_tc_min^2 entries if less;
+    // thinner ones (the look-ahead strips, the last small updates) stay on the
+    // FP32 FMA kernel, whose launch costs less than the tensor-core kernel's
+    // set-up.
+    const uint64_t tc_area = std::min<uint64_t>(uint64_t(2) * h->num_sms * kTcTile * kTcTile,
+                                                uint64_t(h->tune.dense_tc_min) * h->tune.dense_tc_min);
+    auto tc_region = [&](uint32_t rows, uint32_t cols) { return tc && uint64_t(rows) * cols * count >= tc_area; };
     auto update = [&](uint32_t k0, uint32_t kb, DenseRegion reg, cudaStream_t s) -> cudaError_t {
         const uint32_t nr = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
         const uint32_t nc = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;

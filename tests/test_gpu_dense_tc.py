@@ -6,7 +6,8 @@ that partial 128 x 128 tiles, a short last panel, the panel pairs of the
 look-ahead (forced with dense_lookahead) and both tail layouts (in place in the
 CSC values, and the gathered buffer of the mesh) are exercised; each must stay
 within the factor tolerance (per-column max-relative difference <= 1e-4) and
-the profile must show the tensor-core kernel, not the FP32 FMA one, ran.
+the profile must show the tensor-core kernel ran (regions of less than
+dense_tc_min^2 entries stay on the FP32 FMA kernel).
 """
 import numpy as np
 import pytest
@@ -64,7 +65,6 @@ def test_tensor_core_update_matches_oracle(name):
     m = lu.stats["dense_tail"]
     assert m >= tune["dense_tc_min"], m
     assert kt["k_dense_update_tc"][1] > 0 and kt["k_dense_pack"][1] > 0, kt
-    assert kt["k_dense_update"][1] == 0, kt
     err = _check(lu)
     print(f"{name}: m={m} max column relative difference {err:.3e}")
     assert err <= FACTOR_TOL, err
