@@ -77,6 +77,23 @@ __device__ __forceinline__ void st_release_gpu(int32_t *p, int32_t v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Bounded wait until *cnt reaches target (at most `limit` polls; a wait that
+// sees another wait's timeout in the status word gives up early).  Returns
+// false on timeout, with DEV_TIMEOUT set.
+__device__ __forceinline__ bool wait_count(const uint32_t *cnt, uint32_t target, uint32_t *status,
+                                           uint32_t limit) {
+    uint32_t spins = 0;
+    while (ld_acquire_gpu(cnt) < target) {
+        if (++spins > limit) {
+            atomicOr(status, DEV_TIMEOUT);
+            return false;
+        }
+        if ((spins & 1023u) == 0 && (ld_acquire_gpu(status) & DEV_TIMEOUT)) return false;
+        __nanosleep(64);
+    }
+    return true;
+}
+
 // First index in [lo, hi] (inclusive, hi is a valid answer) with a[idx] >= key.
 __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t lo,
                                                     uint32_t hi, uint32_t key) {

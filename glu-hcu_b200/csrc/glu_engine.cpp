@@ -194,6 +194,8 @@ struct glu_handle_s {
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
     DevBuf d_ss_map[2], d_ss_meta[2], d_ss_small[2];  // supernodal L and U sweeps
+    DevBuf d_ss_woff[2], d_ss_widx[2], d_ss_roff[2], d_ss_ridx[2], d_ss_indeg[2];  // their fused form
+    DevBuf d_sweep_done;  // per value set and supernode: releases received (fused sweeps)
     std::vector<SnSweepLevel> ss_levels[2];
     // solve plan
     DevBuf d_sw_cols[4], d_sw_lptr[4], d_sw_ioff[4], d_tail_row_start, d_xo;
@@ -649,6 +651,65 @@ Status build_sn_plan(glu_handle_s *h) {
                 smap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(8, ssmall.size() - g))));
             h->ss_levels[u].push_back(SnSweepLevel{b0, uint32_t(smap.size()) - b0});
         }
+        // fused form: per block the supernodes it solves (waits for) and the
+        // supernodes whose unknowns its scatter updates (releases)
+        std::vector<uint32_t> pos_of(ns);  // supernode -> sweep-order index
+        for (uint32_t i = 0; i < ns; ++i) pos_of[ord[i]] = i;
+        std::vector<uint32_t> woff(1, 0), widx, roff(1, 0), ridx, indeg(ns, 0), mark(ns, UINT32_MAX);
+        auto release_rows = [&](uint32_t blk, uint32_t p0, uint32_t p1, bool by_csc_row) {
+            // targets of the entries [p0, p1): rows of column entries (CSC)
+            for (uint32_t p = p0; p < p1; ++p) {
+                const uint32_t r = s.sym_r_idx[p];
+                (void)by_csc_row;
+                if (r >= t) continue;  // tail rows: solved by a later launch
+                const uint32_t q = pos_of[sn_of[r]];
+                if (mark[q] != blk) {
+                    mark[q] = blk;
+                    ridx.push_back(q);
+                    ++indeg[q];
+                }
+            }
+        };
+        for (uint32_t blk = 0; blk < uint32_t(smap.size()); ++blk) {
+            const uint2 bi = smap[blk];
+            std::vector<uint32_t> mine;
+            if (bi.y & kSnSmallFlag) {
+                for (uint32_t g = 0; g < (bi.y & ~kSnSmallFlag); ++g) mine.push_back(ssmall[bi.x + g]);
+            } else {
+                mine.push_back(bi.x);
+            }
+            for (uint32_t i : mine) widx.push_back(i);
+            woff.push_back(uint32_t(widx.size()));
+            for (uint32_t i : mine) {
+                const uint32_t q = ord[i];
+                const uint32_t s0 = first[q], w = first[q + 1] - s0, last = first[q + 1] - 1;
+                const bool part_all = bi.y & kSnSmallFlag;
+                if (!u) {
+                    // L21 rows of this block: all (small) or the block's chunk of kSnSweepRows
+                    const uint32_t lb = s.l_col_ptr[last] + 1, m = nl(last);
+                    const uint32_t r0 = part_all ? 0 : bi.y * kSnSweepRows, r1 = part_all ? m : std::min(m, r0 + kSnSweepRows);
+                    release_rows(blk, lb + r0, lb + r1, true);
+                } else {
+                    // entries above the block in the supernode's columns, in column order
+                    uint32_t e = 0;
+                    const uint32_t e0 = part_all ? 0 : bi.y * kSnSweepAbove, e1 = part_all ? UINT32_MAX : e0 + kSnSweepAbove;
+                    for (uint32_t c = s0; c <= last; ++c) {
+                        const uint32_t p0 = s.sym_c_ptr[c], p1 = s.l_col_ptr[c] - (c - s0);
+                        const uint32_t cnt = p1 - p0;
+                        const uint32_t lo = std::max(e, e0), hi = std::min(e + cnt, e1);
+                        if (lo < hi) release_rows(blk, p0 + (lo - e), p0 + (hi - e), true);
+                        e += cnt;
+                    }
+                    (void)w;
+                }
+            }
+            roff.push_back(uint32_t(ridx.size()));
+        }
+        GLU_CUDA(upload(h->d_ss_woff[u], woff), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_widx[u], widx), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_roff[u], roff), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_ridx[u], ridx), "upload solve plan");
+        GLU_CUDA(upload(h->d_ss_indeg[u], indeg), "upload solve plan");
         GLU_CUDA(upload(h->d_ss_small[u], ssmall), "upload solve plan");
         GLU_CUDA(upload(h->d_ss_map[u], smap), "upload solve plan");
         GLU_CUDA(upload(h->d_ss_meta[u], smeta), "upload solve plan");
@@ -658,6 +719,14 @@ Status build_sn_plan(glu_handle_s *h) {
         pl.small = h->d_ss_small[u].as<uint32_t>();
         pl.levels = h->ss_levels[u].data();
         pl.nlev = uint32_t(h->ss_levels[u].size());
+        pl.fused = h->tune.sn_sweep_fused;
+        pl.nblocks = uint32_t(smap.size());
+        pl.ns = ns;
+        pl.wait_off = h->d_ss_woff[u].as<uint32_t>();
+        pl.wait_idx = h->d_ss_widx[u].as<uint32_t>();
+        pl.rel_off = h->d_ss_roff[u].as<uint32_t>();
+        pl.rel_idx = h->d_ss_ridx[u].as<uint32_t>();
+        pl.indeg = h->d_ss_indeg[u].as<uint32_t>();
         h->stats.sn_sweep_levels += pl.nlev;
     }
     h->stats.sn_update_flops = upd_flops;
@@ -866,7 +935,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 1u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -1002,6 +1071,11 @@ Status solve_inplace(glu_handle_s *h, uint32_t z, uint32_t count, float *y, uint
     B.vstride = h->nnz;
     B.dstride = h->dense_buffer ? uint64_t(h->m) * h->m : h->nnz;
     B.dinv = h->m ? h->d_dinv.as<float>() + size_t(z) * dinv_per_set(h) : nullptr;
+    if (h->tune.sn_sweep_fused && h->use_sn) {
+        const size_t ns = std::max(h->S.sn[0].ns, h->S.sn[1].ns);
+        GLU_CUDA(h->d_sweep_done.ensure(sizeof(uint32_t) * ns * count + 4), "allocate sweep counters");
+        B.sweep_done = h->d_sweep_done.as<uint32_t>();
+    }
     GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs * count), "allocate solve buffer");
     float *xo = h->d_xo.as<float>();
     const SolvePlanDev S = solve_plan(h);

@@ -182,6 +182,15 @@ struct SnSweepPlan {
     const uint32_t *small = nullptr;  // small supernodes, grouped eight to a block
     const SnSweepLevel *levels = nullptr;  // host array
     uint32_t nlev = 0;
+    // One launch for the whole sweep (fused != 0): blocks take tickets in map
+    // order (levels ascending), block k waits until done[q] == indeg[q] for
+    // the supernodes q = wait_idx[wait_off[k] ..] it solves, and after its
+    // scatter adds one to done[q] for q = rel_idx[rel_off[k] ..], the
+    // supernodes whose unknowns it updated.
+    uint32_t fused = 0;
+    uint32_t nblocks = 0, ns = 0;
+    const uint32_t *wait_off = nullptr, *wait_idx = nullptr, *rel_off = nullptr, *rel_idx = nullptr;
+    const uint32_t *indeg = nullptr;
 };
 constexpr uint32_t kSnSweepRows = 256;    // L21 rows per block of the L sweep
 constexpr uint32_t kSnSweepAbove = 1024;  // U entries per block of the U sweep
@@ -194,6 +203,7 @@ struct SolveBatch {
     uint64_t vstride = 0;
     uint64_t dstride = 0;
     const float *dinv = nullptr;  // inverses of the dense tail's diagonal blocks of the first set
+    uint32_t *sweep_done = nullptr;  // count x (supernodes) counters of the fused sweeps (null: per level)
 };
 // Inverses of the 64 x 64 diagonal blocks of the dense tail's L and U, per
 // value set: dinv[z][b][0: L, 1: U][64 x 64] (row-major), from the factors.
@@ -217,7 +227,8 @@ struct SolvePlanDev {
 // Supernodal sweep over the columns [0, t) (forward L, or backward U), then
 // y[0, t) = xo[0, t).
 cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
-                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, cudaStream_t st);
+                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, uint32_t *done, uint32_t *ticket,
+                         uint32_t *status, uint32_t spin_limit, cudaStream_t st);
 
 // Transform in: y[j] = rhs[col_perm[piv[j]]] * (mc64 ? col_scale_perm[piv[j]] : 1)
 // (symbolic.cc:215-223); out: x[j] = y[row_perm_inv[j]] * (mc64 ? row_scale[j] : 1)

@@ -29,21 +29,6 @@ namespace cg = cooperative_groups;
 
 namespace glu {
 
-// Bounded wait until *cnt reaches target (at most `limit` polls).  Returns
-// false on timeout.
-__device__ __forceinline__ bool wait_count(const uint32_t *cnt, uint32_t target, uint32_t *status,
-                                           uint32_t limit) {
-    uint32_t spins = 0;
-    while (ld_acquire_gpu(cnt) < target) {
-        if (++spins > limit) {
-            atomicOr(status, DEV_TIMEOUT);
-            return false;
-        }
-        if ((spins & 1023u) == 0 && (ld_acquire_gpu(status) & DEV_TIMEOUT)) return false;
-        __nanosleep(64);
-    }
-    return true;
-}
 
 // ------------------------------------------------------------ sparse sweeps --
 // Every sweep is in scatter form: once x_j is final, the entries of its
@@ -429,7 +414,8 @@ static cudaError_t tail_coupling(const DevPattern &P, const SolvePlanDev &S, con
 cudaError_t solve_lower_unit(const DevPattern &P, const SolvePlanDev &S, const float *val,
                              const float *dval, float *y, float *xo, uint32_t nrhs, uint32_t *counters,
                              uint32_t *ticket, uint32_t *status, const SolveBatch &B, cudaStream_t st) {
-    cudaError_t e = S.sn[0].nlev ? run_sn_sweep(P, S.sn[0], false, S.t, val, y, xo, nrhs, B, st)
+    cudaError_t e = S.sn[0].nlev ? run_sn_sweep(P, S.sn[0], false, S.t, val, y, xo, nrhs, B, B.sweep_done, ticket,
+                                                status, S.spin_limit, st)
                                  : run_sweep<SWEEP_L>(P, S, val, y, xo, nrhs, B, st);
     if (e != cudaSuccess) return e;
     return dense_sweep<0>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
@@ -441,7 +427,8 @@ cudaError_t solve_upper(const DevPattern &P, const SolvePlanDev &S, const float 
     cudaError_t e = dense_sweep<1>(S, dval, y, P.n, nrhs, counters, ticket, status, B, st);
     if (e == cudaSuccess) e = tail_coupling(P, S, val, y, nrhs, false, B, st);
     if (e == cudaSuccess)
-        e = S.sn[1].nlev ? run_sn_sweep(P, S.sn[1], true, S.t, val, y, xo, nrhs, B, st)
+        e = S.sn[1].nlev ? run_sn_sweep(P, S.sn[1], true, S.t, val, y, xo, nrhs, B, B.sweep_done, ticket, status,
+                                        S.spin_limit, st)
                          : run_sweep<SWEEP_U>(P, S, val, y, xo, nrhs, B, st);
     return e;
 }

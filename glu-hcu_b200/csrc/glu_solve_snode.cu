@@ -114,20 +114,56 @@ __device__ __forceinline__ void sn_sweep_u_small(const DevPattern &P, const SnSw
         if (ev && xe != 0.0f) atomicAdd(yq + tg, -__fmul_rn(ue, xe));
     }
 }
+// Fused sweeps: the block's item from a ticket in dispatch order, and a
+// wait (thread 0, bounded) until every supernode it solves has received all
+// its releases.  Returns the map index, or UINT32_MAX when the ticket is past
+// the end.  Per-level launches use b0 + blockIdx.x instead.
+__device__ __forceinline__ uint32_t sweep_block(const SnSweepPlan &W, uint32_t b0, const uint32_t *done,
+                                                uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
+    if (!done) return b0 + blockIdx.x;
+    __shared__ uint32_t s_blk;
+    if (threadIdx.x == 0) {
+        uint32_t k = atomicAdd(ticket + blockIdx.z, 1u);
+        if (k < W.nblocks)
+            for (uint32_t e = W.wait_off[k]; e < W.wait_off[k + 1]; ++e) {
+                const uint32_t q = W.wait_idx[e];
+                wait_count(done + q, W.indeg[q], status, spin_limit);
+            }
+        s_blk = k;
+    }
+    __syncthreads();
+    return s_blk < W.nblocks ? s_blk : UINT32_MAX;
+}
+
+// After the block's scatter: one release for every supernode it updated (its
+// atomics are made visible first: barrier, then a device-scope fence).
+__device__ __forceinline__ void sweep_release(const SnSweepPlan &W, uint32_t blk, uint32_t *done) {
+    if (!done) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        for (uint32_t e = W.rel_off[blk]; e < W.rel_off[blk + 1]; ++e) atomicAdd(done + W.rel_idx[e], 1u);
+    }
+}
 }  // namespace
 
 __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
-                                                    uint64_t vstride, uint64_t ystride) {
+                                                    uint64_t vstride, uint64_t ystride, uint32_t *done,
+                                                    uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
     val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
     y += blockIdx.z * ystride;
     xo += blockIdx.z * ystride;
+    if (done) done += size_t(blockIdx.z) * W.ns;
+    const uint32_t blk = sweep_block(W, b0, done, ticket, status, spin_limit);
+    if (blk == UINT32_MAX) return;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
-    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint2 bi = W.map[blk];
     if (bi.y & kSnSmallFlag) {  // a group of small supernodes, one per warp
         const uint32_t wi = threadIdx.x >> 5;
         if (wi < (bi.y & ~kSnSmallFlag)) sn_sweep_l_small(P, W, val, y, xo, nrhs, W.small[bi.x + wi], threadIdx.x & 31);
+        sweep_release(W, blk, done);
         return;
     }
     const uint4 md = W.meta[bi.x];
@@ -191,21 +227,27 @@ __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan
         }
         __syncthreads();
     }
+    sweep_release(W, blk, done);
 }
 
 __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
-                                                    uint64_t vstride, uint64_t ystride) {
+                                                    uint64_t vstride, uint64_t ystride, uint32_t *done,
+                                                    uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
     val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
     y += blockIdx.z * ystride;
     xo += blockIdx.z * ystride;
+    if (done) done += size_t(blockIdx.z) * W.ns;
+    const uint32_t blk = sweep_block(W, b0, done, ticket, status, spin_limit);
+    if (blk == UINT32_MAX) return;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
     __shared__ uint32_t pre[kSnMaxWidth + 1];
-    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint2 bi = W.map[blk];
     if (bi.y & kSnSmallFlag) {  // a group of small supernodes, one per warp
         const uint32_t wi = threadIdx.x >> 5;
         if (wi < (bi.y & ~kSnSmallFlag)) sn_sweep_u_small(P, W, val, y, xo, nrhs, W.small[bi.x + wi], threadIdx.x & 31);
+        sweep_release(W, blk, done);
         return;
     }
     const uint32_t s = W.meta[bi.x].x, w = W.meta[bi.x].y, t = bi.y;
@@ -312,6 +354,7 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
         }
         __syncthreads();
     }
+    sweep_release(W, blk, done);
 }
 
 __global__ void k_sn_copy(const float *__restrict__ xo, float *y, uint32_t t, uint32_t n) {
@@ -320,16 +363,33 @@ __global__ void k_sn_copy(const float *__restrict__ xo, float *y, uint32_t t, ui
 }
 
 cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, uint32_t t, const float *val,
-                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, cudaStream_t st) {
+                         float *y, float *xo, uint32_t nrhs, const SolveBatch &B, uint32_t *done, uint32_t *ticket,
+                         uint32_t *status, uint32_t spin_limit, cudaStream_t st) {
     const uint64_t ystride = uint64_t(nrhs) * P.n;
-    for (uint32_t l = 0; l < W.nlev; ++l) {
-        const SnSweepLevel &lv = W.levels[l];
-        if (lv.blocks == 0) continue;
-        const dim3 grid(lv.blocks, 1, B.count);
+    if (W.fused && done && W.nblocks) {
+        // one launch: blocks in map order by ticket, supernodes wait for their releases
+        cudaError_t e = cudaMemsetAsync(done, 0, sizeof(uint32_t) * size_t(W.ns) * B.count, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(ticket, 0, sizeof(uint32_t) * B.count, st);
+        if (e != cudaSuccess) return e;
+        const dim3 grid(W.nblocks, 1, B.count);
         if (upper)
-            k_sn_sweep_u<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride);
+            k_sn_sweep_u<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, 0, B.vstride, ystride, done, ticket, status,
+                                               spin_limit);
         else
-            k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride);
+            k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, 0, B.vstride, ystride, done, ticket, status,
+                                               spin_limit);
+    } else {
+        for (uint32_t l = 0; l < W.nlev; ++l) {
+            const SnSweepLevel &lv = W.levels[l];
+            if (lv.blocks == 0) continue;
+            const dim3 grid(lv.blocks, 1, B.count);
+            if (upper)
+                k_sn_sweep_u<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride, nullptr,
+                                                   nullptr, status, spin_limit);
+            else
+                k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride, nullptr,
+                                                   nullptr, status, spin_limit);
+        }
     }
     if (t > 0) {  // the vectors of all value sets are contiguous: nrhs * count of them
         uint32_t bx = (t + 255) / 256;

@@ -294,6 +294,9 @@ typedef struct {
     uint32_t dense_rate;       /* dense-block throughput (GFLOP/s) the split cost
                                   model assumes; 0: built in (FMA or tensor-core
                                   rate, whichever the block would use)           */
+    uint32_t sn_sweep_fused;   /* 1: each supernodal solve sweep is one launch in
+                                  which a supernode waits (bounded) for the ones
+                                  that update it; 0: one launch per sweep level  */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);
