@@ -139,13 +139,13 @@ __device__ __forceinline__ void sn_diag_small(const DevPattern &P, const SnPlanD
 }
 
 // Row r of L21 for a supernode of width w <= N <= kTriChunk: x U11 = a in
-// registers (U11 row-major in sM).
+// registers (U11 row-major in sM); a was loaded into xr beforehand.
 template <int N>
 __device__ __forceinline__ void sn_l21_chunk(float *__restrict__ val, const uint32_t *sOff, uint32_t w, uint32_t r,
-                                             const float *sM) {
+                                             const float *sM, const float (&xr)[kTriChunk]) {
     float x[N];
 #pragma unroll
-    for (int c = 0; c < N; ++c) x[c] = uint32_t(c) < w ? ld_cg(val + sOff[c] + r) : 0.0f;
+    for (int c = 0; c < N; ++c) x[c] = xr[c];
     tri_chunk_solve<true>(x, sM, 0, w);
 #pragma unroll
     for (int c = 0; c < N; ++c)
@@ -340,6 +340,15 @@ __global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, S
     const bool lrows = t < nLb;
     if (tid < w) sOff[tid] = P.diag[d.s + tid];
     __syncthreads();
+    // This thread's row of A21 (w <= kTriChunk) does not depend on the
+    // diagonal block: its loads are issued first.
+    const uint32_t rr = t * kSnPanelThreads + tid;
+    float xr[kTriChunk];
+    if (lrows && w <= uint32_t(kTriChunk) && rr < d.m) {
+#pragma unroll
+        for (int c = 0; c < kTriChunk; ++c)
+            xr[c] = uint32_t(c) < w ? ld_cg(val + sOff[c] + (d.l + 1 - (d.s + c)) + rr) : 0.0f;
+    }
     // the factored diagonal block, eight independent loads in flight per thread:
     // L21 blocks keep U11 row-major (leading dimension kTriML), U12 blocks L11
     // column-major (leading dimension kLD)
@@ -373,13 +382,13 @@ __global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, S
         const uint32_t r = t * kSnPanelThreads + tid;
         if (r >= d.m) return;
         if (w <= 2) {
-            sn_l21_chunk<2>(val, sOff, w, r, sF);
+            sn_l21_chunk<2>(val, sOff, w, r, sF, xr);
         } else if (w <= 4) {
-            sn_l21_chunk<4>(val, sOff, w, r, sF);
+            sn_l21_chunk<4>(val, sOff, w, r, sF, xr);
         } else if (w <= 8) {
-            sn_l21_chunk<8>(val, sOff, w, r, sF);
+            sn_l21_chunk<8>(val, sOff, w, r, sF, xr);
         } else if (w <= uint32_t(kTriChunk)) {
-            sn_l21_chunk<kTriChunk>(val, sOff, w, r, sF);
+            sn_l21_chunk<kTriChunk>(val, sOff, w, r, sF, xr);
         } else {
             for (uint32_t c = 0; c < w; ++c) sW[c * kSnPW + tid] = ld_cg(val + sOff[c] + r);
             tri_rows_solve<true>(sW, kSnPW, tid, sF, w);
