@@ -410,16 +410,20 @@ __global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, S
 // in column order, C is stored.  Target positions come from the precomputed
 // table S.pos when present, else from a search in column j's rows.
 __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
-                                                      uint32_t b0, uint32_t atomic) {
+                                                      uint32_t b0, uint32_t atomic, uint32_t count, uint32_t zpb) {
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
     __shared__ __align__(16) float sU[kSnMaxWidth][kTLd];
     __shared__ uint32_t sOff[kSnMaxWidth];
     __shared__ uint32_t sPl[kTile], sLen[kTile], sEx[kTile];
-    float *val = val_base + blockIdx.z * stride;
+    // value sets [z0, z1) of this block: the tile's metadata and target
+    // positions are the same for all of them and computed once
+    const uint32_t z0 = blockIdx.z * zpb, z1 = min(z0 + zpb, count);
     const uint2 bi = S.umap[b0 + blockIdx.x];
     if (bi.y & kSnSmallFlag) {  // small supernodes, one per warp
         const uint32_t wi = threadIdx.x >> 5;
-        if (wi < (bi.y & ~kSnSmallFlag)) sn_update_small(P, S, val, S.usmall[bi.x + wi], atomic != 0, threadIdx.x & 31);
+        if (wi < (bi.y & ~kSnSmallFlag))
+            for (uint32_t z = z0; z < z1; ++z)
+                sn_update_small(P, S, val_base + z * stride, S.usmall[bi.x + wi], atomic != 0, threadIdx.x & 31);
         return;
     }
     const uint32_t i = bi.x, t = bi.y;
@@ -460,15 +464,6 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
         sEx[tid] = ex;
     }
     __syncthreads();
-    for (uint32_t e = tid; e < w * kTile; e += blockDim.x) {
-        const uint32_t k = e / kTile, r = e - k * kTile;
-        sL[k][r] = (r0 + r < d.m) ? ld_cg(val + sOff[k] + r) : 0.0f;
-    }
-    for (uint32_t e = tid; e < w * kTile; e += blockDim.x) {
-        const uint32_t jt = e / w, k = e - jt * w;
-        sU[k][jt] = (k + sLen[jt] >= w) ? ld_cg(val + sPl[jt] - (w - 1 - k)) : 0.0f;
-    }
-    float acc[4][4];
     if (!S.pos) {
         uint32_t rowid[4];
         const uint32_t lbase = P.diag[d.l] + 1;
@@ -494,6 +489,18 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
             }
         }
     }
+    for (uint32_t z = z0; z < z1; ++z) {
+    float *val = val_base + z * stride;
+    if (z > z0) __syncthreads();  // the previous value set's operands are read
+    for (uint32_t e = tid; e < w * kTile; e += blockDim.x) {
+        const uint32_t k = e / kTile, r = e - k * kTile;
+        sL[k][r] = (r0 + r < d.m) ? ld_cg(val + sOff[k] + r) : 0.0f;
+    }
+    for (uint32_t e = tid; e < w * kTile; e += blockDim.x) {
+        const uint32_t jt = e / w, k = e - jt * w;
+        sU[k][jt] = (k + sLen[jt] >= w) ? ld_cg(val + sPl[jt] - (w - 1 - k)) : 0.0f;
+    }
+    float acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -530,6 +537,7 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
             for (int bb = 0; bb < 4; ++bb)
                 if (pos[a][bb] != 0xffffffffu) st_cg(val + pos[a][bb], acc[a][bb]);
     }
+    }  // value sets
 }
 
 // Target metadata, one thread per (supernode, target) pair g (level order,
@@ -603,7 +611,11 @@ cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val,
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                              uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_update<<<dim3(blocks, 1, count), 256, 0, st>>>(P, S, val, stride, b0, atomic);
+    // several value sets per block once the grid has enough blocks without them
+    uint32_t zpb = 1;
+    while (zpb < 8 && zpb * 2 <= count && uint64_t(blocks) * ((count + zpb * 2 - 1) / (zpb * 2)) >= 4ull * 148 * 5)
+        zpb *= 2;
+    k_sn_update<<<dim3(blocks, 1, (count + zpb - 1) / zpb), 256, 0, st>>>(P, S, val, stride, b0, atomic, count, zpb);
     return cudaGetLastError();
 }
 
