@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "glu_internal.h"
 #include "glu_kernels.h"
 
@@ -45,6 +47,14 @@ static Status cuda_fail(cudaError_t e, const char *what) {
         cudaError_t e_ = (call);                              \
         if (e_ != cudaSuccess) return cuda_fail(e_, (what));  \
     } while (0)
+
+// An NVTX range around a public call: the calls appear by name on a profiler
+// timeline (Nsight Systems, ncu's NVTX filters); without a tool attached the
+// push and pop return at once.
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+};
 
 // Device allocations still to fail (GLU_INJECT_ALLOC_FAILURES).
 static std::atomic<int> g_fail_allocs{0};
@@ -935,7 +945,8 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 1u};
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 1u,
+                         0u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -1223,6 +1234,7 @@ glu_status glu_predict_lu(glu_symbolic_t s, const double *ax, float *val) {
 void glu_symbolic_destroy(glu_symbolic_t s) { delete s; }
 
 glu_status glu_create(glu_symbolic_t s, int device, uint32_t batch, glu_handle_t *out) {
+    TraceRange trace_("glu_create");
     if (!s) return set_error(GLU_ERR_ARG, "null symbolic handle");
     SymbolicData copy = s->s;
     return create_handle(device, std::move(copy), batch, out);
@@ -1481,7 +1493,8 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
                            "factor (supernode panels)");
             if (lv.ublocks)
                 GLU_LAUNCH(KK_SN_UPDATE,
-                           launch_sn_update(h->P, h->SN, val, stride, count, lv.ub0, lv.ublocks, lv.atomic, st),
+                           launch_sn_update(h->P, h->SN, val, stride, count, lv.ub0, lv.ublocks, lv.atomic,
+                                            h->tune.batch_tile, st),
                            "factor (supernode updates)");
         }
     }
@@ -1688,6 +1701,7 @@ Status factor_finish(glu_handle_s *h, int perturb) {
 extern "C" {
 
 glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int perturb, glu_stream stream) {
+    TraceRange trace_("glu_factor");
     if (!h) return set_error(GLU_ERR_ARG, "null handle");
     Status s = check_range(h, first, count);
     if (s != GLU_OK) return s;
@@ -1701,6 +1715,7 @@ glu_status glu_factor(glu_handle_t h, uint32_t first, uint32_t count, int pertur
 
 glu_status glu_factor_many(uint32_t count, const glu_handle_t *handles, int perturb, const glu_stream *streams,
                            uint32_t nstreams) {
+    TraceRange trace_("glu_factor_many");
     if (count == 0) return GLU_OK;
     if (!handles || (nstreams && !streams)) return set_error(GLU_ERR_ARG, "null argument");
     for (uint32_t i = 0; i < count; ++i)
@@ -1733,6 +1748,7 @@ glu_status glu_factor_many(uint32_t count, const glu_handle_t *handles, int pert
 
 glu_status glu_solve(glu_handle_t h, uint32_t inst, uint32_t nrhs, const float *b, float *x,
                      glu_memory where, glu_stream stream) {
+    TraceRange trace_("glu_solve");
     if (!h) return set_error(GLU_ERR_ARG, "null handle");
     return solve_f32(h, inst, nrhs, b, x, where, false, S_(stream));
 }
@@ -1891,6 +1907,7 @@ extern "C" {
 glu_status glu_solve_refined(glu_handle_t h, uint32_t first, uint32_t count, uint32_t nrhs,
                              const double *b, double *x, double tol, uint32_t maxit, int transposed,
                              glu_memory where, glu_refine_stats *stats, glu_stream stream) {
+    TraceRange trace_("glu_solve_refined");
     if (!h || !b || !x) return set_error(GLU_ERR_ARG, "null argument");
     Status s = check_range(h, first, count);
     if (s != GLU_OK) return s;
@@ -1923,6 +1940,7 @@ glu_status glu_solve_refined_many(uint32_t count, const glu_handle_t *handles, c
                                   const double *const *b, double *const *x, double tol, uint32_t maxit,
                                   glu_memory where, glu_refine_stats *stats, const glu_stream *streams,
                                   uint32_t nstreams) {
+    TraceRange trace_("glu_solve_refined_many");
     if (count == 0) return GLU_OK;
     if (!handles || !nrhs || !b || !x || (nstreams && !streams)) return set_error(GLU_ERR_ARG, "null argument");
     std::vector<RefineJob> jobs(count);

@@ -24,6 +24,8 @@
 // column order (fused multiply-add instead of multiply and subtract; the L21
 // rows of supernodes wider than one are multiplied by the pivot's correctly
 // rounded reciprocal instead of divided by the pivot).
+#include <algorithm>
+
 #include "glu_common.cuh"
 #include "glu_kernels.h"
 #include "glu_tri.cuh"
@@ -609,12 +611,16 @@ cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val,
 }
 
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                             uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st) {
+                             uint32_t b0, uint32_t blocks, uint32_t atomic, uint32_t batch_tile, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    // several value sets per block once the grid has enough blocks without them
+    // several value sets per block once the grid has enough blocks without
+    // them (or batch_tile of them when set)
     uint32_t zpb = 1;
-    while (zpb < 8 && zpb * 2 <= count && uint64_t(blocks) * ((count + zpb * 2 - 1) / (zpb * 2)) >= 4ull * 148 * 5)
-        zpb *= 2;
+    if (batch_tile)
+        zpb = std::min(batch_tile, count);
+    else
+        while (zpb < 8 && zpb * 2 <= count && uint64_t(blocks) * ((count + zpb * 2 - 1) / (zpb * 2)) >= 4ull * 148 * 5)
+            zpb *= 2;
     k_sn_update<<<dim3(blocks, 1, (count + zpb - 1) / zpb), 256, 0, st>>>(P, S, val, stride, b0, atomic, count, zpb);
     return cudaGetLastError();
 }

@@ -71,7 +71,7 @@ cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, 
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                             const float *pert_z, uint32_t b0, uint32_t blocks, uint32_t max_width, cudaStream_t st);
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
-                             uint32_t b0, uint32_t blocks, uint32_t atomic, cudaStream_t st);
+                             uint32_t b0, uint32_t blocks, uint32_t atomic, uint32_t batch_tile, cudaStream_t st);
 // Setup, once per pattern: the target metadata (S.meta, S.tgt_off set), then
 // the position table (S.tgt set).
 cudaError_t launch_sn_targets(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint4 *tgt, cudaStream_t st);

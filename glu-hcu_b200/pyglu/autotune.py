@@ -16,7 +16,9 @@ factorization path in use reads --
   block), the width from which the dense block takes its panels in
   look-ahead pairs, the width from which it updates on the tensor cores;
 * column path (sn_width = 0): lanes per update, the cluster size of the
-  narrow-level kernel, the work that sends a level to its own launch.
+  narrow-level kernel, the work that sends a level to its own launch;
+* batched handles, in addition: the batch tile, the number of value sets one
+  supernode-update block applies its tile to.
 
 Each knob takes its values in turn with the others held; the fastest
 refactorization (median of ``repeats``) is kept; two passes.
@@ -92,10 +94,15 @@ def _time(lu, values, repeats):
     return float(np.median(times))
 
 
-def _space_for(cfg, space):
+# the batch tile (value sets per supernode-update block), for batched handles
+BATCH_SPACE = {"batch_tile": [0, 1, 2, 4, 8, 16]}
+
+
+def _space_for(cfg, space, batch=1):
     if space is not None:
         return space
-    return SUPERNODAL_SPACE if cfg.get("sn_width", 1) else COLUMN_SPACE
+    base = SUPERNODAL_SPACE if cfg.get("sn_width", 1) else COLUMN_SPACE
+    return {**base, **BATCH_SPACE} if batch > 1 else base
 
 
 def tune(lu, data=None, repeats=3, cache=DEFAULT_CACHE, space=None, use_cache=True, passes=2):
@@ -128,7 +135,7 @@ def tune(lu, data=None, repeats=3, cache=DEFAULT_CACHE, space=None, use_cache=Tr
     best = dict(base)
     best_ms = _time(lu, values, repeats)
     report = {"default_ms": best_ms, "trials": [], "cached": False}
-    grid = _space_for(base, space)
+    grid = _space_for(base, space, batch)
     for _ in range(passes):
         improved = False
         for knob, choices in grid.items():

@@ -297,6 +297,9 @@ typedef struct {
     uint32_t sn_sweep_fused;   /* 1: each supernodal solve sweep is one launch in
                                   which a supernode waits (bounded) for the ones
                                   that update it; 0: one launch per sweep level  */
+    uint32_t batch_tile;       /* value sets one supernode-update block applies
+                                  its tile to (its metadata and target positions
+                                  computed once); 0: chosen from the grid size */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);
