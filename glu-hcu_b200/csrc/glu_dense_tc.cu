@@ -62,6 +62,7 @@ constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A0, A1, A2, B0, B1, 
 constexpr int kThreads = 192;                            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 constexpr uint32_t kTmemCols = 4 * kTile;                // two pairs (big, small) of FP32 accumulators
 constexpr size_t kBarBytes = 256;
+constexpr int kRing = 4;  // tile ids in flight between the producer and the other roles
 constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + 1024;  // + alignment slack
 
 // Instruction descriptor of tcgen05.mma kind::tf32: D FP32 (bits 4-5 = 1), A
@@ -248,7 +249,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_dense_update_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       float *val_base, uint64_t stride, const uint32_t *__restrict__ doff, uint32_t m, uint32_t r0,
                       uint32_t nchunks, DenseRegion reg, uint32_t tiles_r, uint32_t tiles_c, uint32_t count,
-                      const float *__restrict__ diag_scratch, uint32_t *status, uint32_t spin_limit) {
+                      const float *__restrict__ diag_scratch, uint32_t *status, uint32_t spin_limit,
+                      uint32_t *tile_counter) {
     extern __shared__ uint8_t tc_smem_raw[];
     uint8_t *smem = tc_smem_raw + ((1024u - (smem_addr(tc_smem_raw) & 1023u)) & 1023u);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + kStages * kStageBytes);
@@ -257,7 +259,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t *acc_full = bars + 2 * kStages;  // [2] accumulator ready (MMA commit)
     uint64_t *acc_empty = acc_full + 2;       // [2] accumulator read (4 epilogue warps)
     uint64_t *done = acc_empty + 2;           // all MMAs of this CTA complete
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    uint64_t *tile_full = done + 1;           // [kRing] tile id written (producer)
+    uint64_t *tile_empty = tile_full + kRing;  // [kRing] tile id read (MMA issuer + 4 epilogue warps)
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tile_empty + kRing);
+    uint32_t *tile_id = tmem_slot + 1;        // [kRing]
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t total = tiles_r * tiles_c * count;
 
@@ -271,6 +276,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&acc_empty[a], 4);
         }
         mbar_init(done, 1);
+        for (int j = 0; j < kRing; ++j) {
+            mbar_init(&tile_full[j], 1);
+            mbar_init(&tile_empty[j], 5);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapB)) : "memory");
@@ -291,7 +300,19 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) {
             uint32_t g = 0;
             bool ok = true;
-            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            // tiles are drawn from a counter shared by all CTAs (a CTA that
+            // starts late takes fewer); each id goes to the other roles through
+            // the ring, the id past the last tile ends their loops
+            for (uint32_t i = 0; ok; ++i) {
+                const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
+                if (!mbar_wait(&tile_empty[slot], sph ^ 1, spin_limit)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t t = atomicAdd(tile_counter, 1u);
+                tile_id[slot] = t < total ? t : total;
+                mbar_arrive(&tile_full[slot]);
+                if (t >= total) break;
                 const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
                 const int ya = int(r0 + tl.rbase), yb = int(r0 + tl.cbase), zz = int(tl.z);
                 for (uint32_t kc = 0; kc < nchunks; ++kc, ++g) {
@@ -323,7 +344,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t g = 0;  // stages consumed
             uint32_t u = 0;  // accumulator rounds: one per (tile, K chunk)
             bool ok = true;
-            for (uint32_t t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            for (uint32_t i = 0; ok; ++i) {
+                const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
+                if (!mbar_wait(&tile_full[slot], sph, spin_limit)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t t = tile_id[slot];
+                mbar_arrive(&tile_empty[slot]);
+                if (t >= total) break;
                 for (uint32_t kc = 0; kc < nchunks; ++kc, ++g, ++u) {
                     const uint32_t a = u & 1, aph = (u >> 1) & 1;
                     const uint32_t s = g % kStages, ph = (g / kStages) & 1;
@@ -377,7 +406,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
         }
         uint32_t u = 0;  // accumulator rounds, as the MMA issuer counts them
-        for (uint32_t t = blockIdx.x; t < total; t += gridDim.x) {
+        for (uint32_t i = 0;; ++i) {
+            const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
+            if (!__all_sync(0xffffffffu, mbar_wait(&tile_full[slot], sph, spin_limit))) {
+                if (lane == 0) atomicOr(status, DEV_TIMEOUT);
+                break;
+            }
+            const uint32_t t = tile_id[slot];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tile_empty[slot]);
+            if (t >= total) break;
             const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
             float *val = val_base + tl.z * stride;
             const bool rok = tl.rbase + row < reg.r_hi;
@@ -489,7 +527,7 @@ cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count,
 cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
                                    uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
                                    const float *diag_scratch, DenseRegion reg, uint32_t *status,
-                                   uint32_t spin_limit, uint32_t num_sms, cudaStream_t st) {
+                                   uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter, cudaStream_t st) {
     static PerDeviceOnce attr;
     cudaError_t e = attr.run([] {
         return cudaFuncSetAttribute(k_dense_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
@@ -505,8 +543,11 @@ cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &m
     uint32_t grid = uint32_t(std::min<uint64_t>(std::max<uint64_t>(total, 1), num_sms));
     if (reg.writeback) grid = std::max<uint32_t>(grid, std::min<uint32_t>(count, num_sms));
     const uint32_t nchunks = (kb + kChunk - 1) / kChunk;
+    e = cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
     k_dense_update_tc<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, val, stride, doff, m, r0, nchunks, reg,
-                                                          tiles_r, tiles_c, count, diag_scratch, status, spin_limit);
+                                                          tiles_r, tiles_c, count, diag_scratch, status, spin_limit,
+                                                          tile_counter);
     return cudaGetLastError();
 }
 

@@ -233,7 +233,7 @@ struct glu_handle_s {
     cudaEvent_t ev_fork = nullptr, ev_panel = nullptr, ev_rest = nullptr;
     // tensor-core dense update: TF32 hi/lo operand packs and their TMA maps
     // (allocated on the first factorization that uses them)
-    DevBuf d_packA, d_packB;
+    DevBuf d_packA, d_packB, d_tc_counter;
     // inverses of the dense tail's 64 x 64 diagonal blocks (L and U) per value
     // set, for the dense triangular solves
     DevBuf d_dinv;
@@ -1549,6 +1549,7 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         GLU_CUDA(h->d_packB.alloc(pack_bytes), "allocate tensor-core operand packs");
         GLU_CUDA(dense_tc_tensor_map(h->d_packA.as<float>(), h->m, h->batch, &h->map_packA), "tensor map");
         GLU_CUDA(dense_tc_tensor_map(h->d_packB.as<float>(), h->m, h->batch, &h->map_packB), "tensor map");
+        GLU_CUDA(h->d_tc_counter.alloc(sizeof(uint32_t) * 2), "allocate tile counters");
         h->pack_m = h->m;
     }
     uint32_t *dstatus = h->d_status.as<uint32_t>();
@@ -1570,8 +1571,10 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         cudaError_t e = pf.begin(s);
         if (e != cudaSuccess) return e;
         if (tc_region(nr, nc)) {
+            // a tile counter per stream (launches on one stream run in order)
+            uint32_t *ctr = h->d_tc_counter.as<uint32_t>() + (s == st ? 0 : 1);
             e = launch_dense_update_tc(h->map_packA, h->map_packB, dbase, dstride, count, doff, h->m, k0, kb, dscr,
-                                       reg, dstatus, h->spin_limit, h->num_sms, s);
+                                       reg, dstatus, h->spin_limit, h->num_sms, ctr, s);
             if (e == cudaSuccess) e = pf.end(KK_UPDATE_TC, s);
         } else {
             e = launch_dense_update(dbase, dstride, count, doff, h->m, k0, kb, dscr, reg, s);

@@ -113,7 +113,7 @@ cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count,
 cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
                                    uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
                                    const float *diag_scratch, DenseRegion reg, uint32_t *status,
-                                   uint32_t spin_limit, uint32_t num_sms, cudaStream_t st);
+                                   uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter, cudaStream_t st);
 // A trailing block that is dense but not completely filled is factored in a
 // separate m x m column-major buffer: gather copies the block's pattern
 // entries of the CSC values into the (zeroed) buffer, scatter copies the
