@@ -583,16 +583,15 @@ Status build_sn_plan(glu_handle_s *h) {
                       h->d_sn_tgt.as<uint4>(),       nullptr,                    h->d_sn_pos_off.as<uint64_t>()};
     GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
     GLU_CUDA(cudaDeviceSynchronize(), "supernode targets");
-    // Position table of the update scatter, when it fits in half of the free
-    // memory (the values of every value set are allocated by now).  Without
-    // it each update entry searches its target column's rows, a chain of
-    // dependent loads per entry that dominates when the targets are long
-    // dense-tail columns.
+    // Position table of the update scatter, when it fits in a quarter of the
+    // free memory (the values of every value set are allocated by now).
+    // Without it an update entry in a complete in-place dense tail computes
+    // its position, any other searches its target column's rows.
     h->d_sn_pos.release();
     const uint64_t entries = pos_off[ns];
     size_t free_b = 0, total_b = 0;
     if (entries > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
-        double(entries) * sizeof(uint32_t) <= 0.5 * double(free_b) &&
+        double(entries) * sizeof(uint32_t) <= 0.25 * double(free_b) &&
         h->d_sn_pos.alloc(sizeof(uint32_t) * entries) == cudaSuccess) {
         GLU_CUDA(launch_sn_positions(h->P, h->SN, ns, h->d_sn_pos.as<uint32_t>(), 0), "supernode positions");
         GLU_CUDA(cudaDeviceSynchronize(), "supernode positions");
@@ -903,6 +902,9 @@ Status build_plan(glu_handle_s *h) {
 
     Status sn = build_sn_plan(h);
     if (sn != GLU_OK) return sn;
+    h->SN.tail_start = h->d_tail_start.as<uint32_t>();
+    h->SN.t = t;
+    h->SN.tail_full = (m > 0 && !h->dense_buffer) ? 1u : 0u;
     uint32_t wide = 0, chains = 0;
     for (auto &st : h->steps) (st.kind == STEP_CHAIN ? chains : wide)++;
     h->stats.wide_levels = h->use_sn ? 0 : wide;

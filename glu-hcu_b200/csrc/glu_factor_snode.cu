@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
     __shared__ __align__(16) float sU[kSnMaxWidth][kTLd];
     __shared__ uint32_t sOff[kSnMaxWidth];
-    __shared__ uint32_t sPl[kTile], sLen[kTile], sEx[kTile];
+    __shared__ uint32_t sPl[kTile], sLen[kTile], sEx[kTile], sJ[kTile];
     // value sets [z0, z1) of this block: the tile's metadata and target
     // positions are the same for all of them and computed once
     const uint32_t z0 = blockIdx.z * zpb, z1 = min(z0 + zpb, count);
@@ -454,16 +454,18 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
     if (tid < w) sOff[tid] = P.diag[d.s + tid] + (d.l + 1 - (d.s + tid)) + r0;
     if (tid < kTile) {
         const uint32_t jt = c0 + tid;
-        uint32_t pl = 0, len = 0, ex = 0;
+        uint32_t pl = 0, len = 0, ex = 0, tj = 0;
         if (jt < d.nt) {
             const uint4 g = S.tgt[S.tgt_off[i] + jt];
             pl = g.x;
             len = g.y;
             ex = g.z;
+            tj = g.w;
         }
         sPl[tid] = pl;
         sLen[tid] = len;
         sEx[tid] = ex;
+        sJ[tid] = tj;
     }
     __syncthreads();
     if (!S.pos) {
@@ -478,14 +480,21 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
         for (int bb = 0; bb < 4; ++bb) {
             const uint32_t jt = tc * 4 + bb;
             const bool tv = sLen[jt] != 0;
-            const uint32_t pl = sPl[jt], ex = sEx[jt];
+            const uint32_t pl = sPl[jt], ex = sEx[jt], tj = sJ[jt];
+            // a complete dense-tail column: tail rows at fixed offsets
+            const bool tcol = S.tail_full && tj >= S.t;
+            const uint32_t ts = tcol ? __ldg(S.tail_start + (tj - S.t)) : 0u;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 const uint32_t r = r0 + tr * 4 + a;
                 uint32_t q = 0xffffffffu;
                 if (tv && r < d.m) {
-                    q = pl + 1 + r;
-                    if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, rowid[a]);
+                    if (tcol && rowid[a] >= S.t) {
+                        q = ts + (rowid[a] - S.t);
+                    } else {
+                        q = pl + 1 + r;
+                        if (ex) q = lower_bound_u32(P.ridx, q, q + ex + 1, rowid[a]);
+                    }
                 }
                 pos[a][bb] = q;
             }
@@ -545,7 +554,8 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
 // Target metadata, one thread per (supernode, target) pair g (level order,
 // S.tgt_off the prefix): {CSC position pl of the supernode's last row l in
 // target column j, rows of the supernode present in column j (0: the column
-// cannot hold the L21 rows), rows of column j below l that are not L21 rows}.
+// cannot hold the L21 rows), rows of column j below l that are not L21 rows,
+// j}.
 __global__ void __launch_bounds__(256) k_sn_targets(DevPattern P, SnPlanDev S, uint32_t nsn, uint4 *tgt) {
     const uint32_t total = S.tgt_off[nsn];
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
@@ -555,7 +565,7 @@ __global__ void __launch_bounds__(256) k_sn_targets(DevPattern P, SnPlanDev S, u
         const uint32_t j = P.cidx[e];
         const uint32_t pl = P.cpos[e];
         const uint32_t below = P.cptr[j + 1] - pl - 1;
-        uint4 o = make_uint4(pl, 0u, 0u, 0u);
+        uint4 o = make_uint4(pl, 0u, 0u, j);
         if (below >= d.m) {  // always, for a pattern closed under fill
             o.y = seg_len(P, j, pl, d.l, d.w);
             o.z = below - d.m;

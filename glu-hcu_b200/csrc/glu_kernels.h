@@ -62,6 +62,12 @@ struct SnPlanDev {
     const uint4 *tgt;         // per target: {CSC position of row l, rows present (0: none), extra rows, 0}
     const uint32_t *pos;      // CSC positions of the update outputs, or nullptr
     const uint64_t *pos_off;  // [count]
+    // When the dense tail [t, n) is complete and factored in place, row i >= t
+    // of tail column j sits at tail_start[j - t] + (i - t): the update computes
+    // those positions instead of searching for them (tail_full != 0).
+    const uint32_t *tail_start = nullptr;
+    uint32_t t = 0;
+    uint32_t tail_full = 0;
 };
 
 // Blocks [b0, b0 + blocks) of one level's diagonal-block, panel or update
