@@ -242,9 +242,15 @@ __device__ __forceinline__ void sn_update_small(const DevPattern &P, const SnPla
         if (ov) g = S.tgt[g0 + jt];
         const bool v = ov && g.y != 0;
         uint32_t q = g.x + 1 + r;
-        if (v && g.z)
-            q = S.pos ? __ldg(S.pos + S.pos_off[i] + uint64_t(jt) * m + r)
-                      : lower_bound_u32(P.ridx, q, q + g.z + 1, __ldg(P.ridx + lbase + r));
+        if (v && g.z) {
+            const uint32_t row = __ldg(P.ridx + lbase + r);
+            if (S.pos)
+                q = __ldg(S.pos + S.pos_off[i] + uint64_t(jt) * m + r);
+            else if (S.tail_full && g.w >= S.t && row >= S.t)  // complete dense-tail column
+                q = __ldg(S.tail_start + (g.w - S.t)) + (row - S.t);
+            else
+                q = lower_bound_u32(P.ridx, q, q + g.z + 1, row);
+        }
         float acc = (v && !atomic) ? ld_cg(val + q) : 0.0f;
 #pragma unroll
         for (int c = 0; c < SW; ++c) {
