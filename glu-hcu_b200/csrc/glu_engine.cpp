@@ -1057,6 +1057,25 @@ Status read_status(glu_handle_s *h, cudaStream_t st, uint32_t *flags) {
     return GLU_OK;
 }
 
+// Kernels one FP32 solve (both triangular sweeps) launches, from the plan.
+uint64_t solve_kernel_count(const glu_handle_s *h, bool trans) {
+    uint64_t k = 0;
+    const SolvePlanDev &S = h->S;
+    for (int u = 0; u < 2; ++u) {
+        const bool sn = !trans && S.sn[u].nlev;
+        if (sn) {
+            uint32_t lev = 0;
+            for (uint32_t l = 0; l < S.sn[u].nlev; ++l) lev += S.sn[u].levels[l].blocks ? 1 : 0;
+            k += (S.sn[u].fused && h->use_sn ? 1 : lev) + (S.t > 0 ? 1 : 0);
+        } else {
+            const int mode = trans ? (u == 0 ? SWEEP_UT : SWEEP_LT) : (u == 0 ? SWEEP_L : SWEEP_U);
+            k += S.sweep[mode].nsteps + ((mode == SWEEP_U || mode == SWEEP_UT) && S.t > 0 ? 1 : 0);
+        }
+    }
+    if (S.m) k += 2 + (S.t > 0 ? 1 : 0);  // two dense sweeps, the tail coupling
+    return k;
+}
+
 // Floats of the dense tail's diagonal-block inverses of one value set.
 size_t dinv_per_set(const glu_handle_s *h) { return size_t((h->m + 63) / 64) * 2 * 64 * 64; }
 
@@ -1096,6 +1115,7 @@ Status solve_inplace(glu_handle_s *h, uint32_t z, uint32_t count, float *y, uint
     GLU_CUDA(h->d_xo.ensure(sizeof(float) * size_t(h->n) * nrhs * count), "allocate solve buffer");
     float *xo = h->d_xo.as<float>();
     const SolvePlanDev S = solve_plan(h);
+    h->stats.solve_launches += solve_kernel_count(h, trans);
     if (!trans) {
         GLU_CUDA(solve_lower_unit(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st), "lower solve");
         GLU_CUDA(solve_upper(h->P, S, val, dval, y, xo, nrhs, cnt, tk, status, B, st), "upper solve");
@@ -1127,6 +1147,7 @@ Status solve_f32(glu_handle_s *h, uint32_t inst, uint32_t nrhs, const float *b, 
     }
     GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), st), "reset status");
     const TransformDev &T = h->T;
+    h->stats.solve_launches = 2;  // the two transforms; solve_inplace adds the sweeps
     GLU_CUDA(launch_transform_f32(trans ? T.tin_idx : T.in_idx, trans ? T.tin_scale : T.in_scale, bin, y,
                                   h->n, nrhs, st), "transform");
     Status s = solve_inplace(h, inst, 1, y, nrhs, trans, st);
@@ -1827,6 +1848,7 @@ Status refine_residual(RefineJob &j) {
     const uint32_t *vmap = j.tr ? h->d_a0_ident.as<uint32_t>() : h->d_a0_vmap.as<uint32_t>();
     const double *ax0 = h->d_ax0.as<double>() + size_t(j.first) * h->nnz_src;
     double *norms = h->d_norms.as<double>();
+    h->stats.solve_launches += 1;
     GLU_CUDA(launch_residual(rptr, cidx, vmap, ax0, h->n, j.bz, j.xz, h->d_r64.as<double>(), j.nvec, j.nrhs,
                              h->nnz_src, norms, j.st),
              "residual");
@@ -1840,6 +1862,7 @@ Status refine_solve(RefineJob &j, const double *src, int accumulate) {
     glu_handle_s *h = j.h;
     const TransformDev &T = h->T;
     float *y = h->d_y.as<float>();
+    h->stats.solve_launches += 2;  // the two transforms
     GLU_CUDA(launch_transform_f64_to_f32(j.tr ? T.tin_idx : T.in_idx, j.tr ? T.tin_scale : T.in_scale, src, y, h->n,
                                          j.nvec, j.st),
              "transform");
@@ -1864,6 +1887,7 @@ Status refine_start(RefineJob &j) {
     }
     double *norms = h->d_norms.as<double>();
     GLU_CUDA(cudaMemsetAsync(h->d_status.p, 0, sizeof(uint32_t), j.st), "reset status");
+    h->stats.solve_launches = 1;  // the norms of b; every solve and residual adds its own
     GLU_CUDA(launch_norms(j.bz, h->n, j.nvec, norms + 2 * j.nvec, j.st), "norms");
     Status s = refine_solve(j, j.bz, 0);
     if (s != GLU_OK) return s;

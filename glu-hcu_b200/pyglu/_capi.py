@@ -75,7 +75,8 @@ class Stats(C.Structure):
                 ("last_factor_ms", C.c_float), ("pert", C.c_float), ("supernodes", C.c_uint32),
                 ("sn_levels", C.c_uint32), ("sn_update_flops", C.c_double), ("sn_update_bytes", C.c_double),
                 ("sn_panel_bytes", C.c_double), ("sn_sweep_levels", C.c_uint32),
-                ("dense_update_bytes", C.c_double), ("dense_update_flops", C.c_double)]
+                ("dense_update_bytes", C.c_double), ("dense_update_flops", C.c_double),
+                ("solve_launches", C.c_uint64)]
 
 
 class Tuning(C.Structure):

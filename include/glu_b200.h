@@ -228,6 +228,8 @@ typedef struct {
                                   C read and written once per launch plus one
                                   FP32 read of the panels' L21 and U12          */
     double dense_update_flops; /* and their flops, 2 K per updated entry        */
+    uint64_t solve_launches;   /* kernel launches of the last solve call (glu_solve,
+                                  glu_solve_transposed, glu_solve_refined)       */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
 
