@@ -11,10 +11,12 @@
 //     a b ~= a0 b0 + (a0 b1 + a1 b0) + (a0 b2 + a1 b1 + a2 b0),
 // whose error, below 2^-32 |a b|, is far under FP32 rounding.  The big term
 // a0 b0 (exact in FP32) and the small terms go to separate FP32 accumulators
-// in tensor memory, so the tensor core's truncating accumulation of the big
-// term runs over four MMAs per 32-wide K chunk and that of the small terms
-// stays 2^-11 below it.  Each chunk's two partial sums are then subtracted from
-// the entry in FP32 with round to nearest, c := (c - big) - small, in K order.
+// in tensor memory over the whole K of the update (16 MMAs of K = 8 for a
+// panel pair), so the small terms' truncating accumulation stays 2^-11 below
+// the big one's; the tile's two sums are then subtracted from the entry in
+// FP32 with round to nearest, c := (c - big) - small.  The big sum takes one
+// truncation per MMA (K / 8 in all; the FMA kernel rounds once per product),
+// and the tile's C is read and written once.
 
 // Data flow per update:
 //   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
@@ -27,12 +29,12 @@
 //        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 32 FP32
 //                 operand boxes (128-byte swizzle), three parts of A and of B
 //                 per 32-wide K chunk, into a 2-stage ring;
-//        warp 1   MMA issuer: 6 x 4 tcgen05.mma (M = N = 128, K = 8) per
-//                 chunk into one of two accumulator pairs (big, small);
+//        warp 1   MMA issuer: 6 tcgen05.mma (M = N = 128, K = 8) per 8 of
+//                 K into one of two accumulator pairs (big, small), the
+//                 pair of the tile before being read meanwhile;
 //        warps 2-5 epilogue: load the C tile from HBM into registers while
-//                 the MMAs run, tcgen05.ld each chunk's two partial sums and
-//                 subtract them, store the tile; the other accumulator pair
-//                 takes the next chunk's MMAs.
+//                 the MMAs run, tcgen05.ld the tile's two sums, subtract
+//                 them, hand the pair back, store the tile.
 //      C stays where it lies (element (i, j) at val[doff[j] + i]), so in-place
 //      tails with irregular column offsets need no copy.
 // All waits on mbarriers are bounded (spin_limit polls); a wait that runs out
@@ -240,6 +242,68 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
     }
 }
 
+// ------------------------------------------------------- coupling pack --
+// Operands of one group of deferred sparse columns (up to 128, slots slot0 ..
+// slot0 + ncols - 1): packA[z][i][128 p + s] = part p of L(t + i, k_s),
+// packB[z][j][128 p + s] = part p of U(k_s, t + j), zero where the pattern has
+// no entry and for slots past the group.  Block b < nblk takes tail rows
+// [128 b, 128 b + 128): thread s walks column k_s's CSC entries
+// [lstart[g][b], lstart[g][b + 1]) (g = slot0 + s), the ones in those rows.
+// Block nblk + b takes tail columns [128 b, 128 b + 128): thread s walks row
+// k_s's CSR entries [ustart[g][b], ustart[g][b + 1]), the ones in those
+// columns (their CSC positions from cpos).  The start tables (nblk + 1 entries
+// per slot) are computed with the plan.  A 128 x 128 tile in shared memory,
+// then coalesced writes of the three parts.
+constexpr uint32_t kCoupleLd = kTile + 1;
+constexpr size_t kCoupleSmem = sizeof(float) * kTile * kCoupleLd;
+
+__global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restrict__ ridx,
+                                                       const uint32_t *__restrict__ cidx,
+                                                       const uint32_t *__restrict__ cpos,
+                                                       const float *__restrict__ val_base, uint64_t stride,
+                                                       uint32_t t, uint32_t m, uint32_t ncols, uint32_t slot0,
+                                                       const uint32_t *__restrict__ lstart,
+                                                       const uint32_t *__restrict__ ustart, uint32_t nblk,
+                                                       float *__restrict__ packA, float *__restrict__ packB) {
+    extern __shared__ float sT[];  // [128][kCoupleLd]: sT[r * kCoupleLd + s]
+    const float *val = val_base + blockIdx.z * stride;
+    const uint32_t tid = threadIdx.x;
+    const bool aside = blockIdx.x < nblk;
+    const uint32_t b = aside ? blockIdx.x : blockIdx.x - nblk, b0 = b * kTile;
+    for (uint32_t e = tid; e < kTile * kCoupleLd; e += kTile) sT[e] = 0.0f;
+    __syncthreads();
+    if (tid < ncols) {
+        const uint32_t *st = (aside ? lstart : ustart) + size_t(slot0 + tid) * (nblk + 1) + b;
+        const uint32_t p0 = __ldg(st), p1 = __ldg(st + 1);
+        if (aside) {
+            for (uint32_t p = p0; p < p1; ++p) sT[(__ldg(ridx + p) - t - b0) * kCoupleLd + tid] = ld_cg(val + p);
+        } else {
+            for (uint32_t e = p0; e < p1; ++e)
+                sT[(__ldg(cidx + e) - t - b0) * kCoupleLd + tid] = ld_cg(val + __ldg(cpos + e));
+        }
+    }
+    __syncthreads();
+    float *pack = aside ? packA : packB;
+    const uint32_t rows = min(uint32_t(kTile), m - b0);
+    for (uint32_t e = tid; e < rows * (kTile / 4); e += kTile) {
+        const uint32_t r = e / (kTile / 4), q = e - r * (kTile / 4);
+        float4 p0, p1, p2;
+        float *a0 = &p0.x, *a1 = &p1.x, *a2 = &p2.x;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float v = sT[r * kCoupleLd + 4 * q + u];
+            a0[u] = tf32_rna(v);
+            const float r1 = v - a0[u];
+            a1[u] = tf32_rna(r1);
+            a2[u] = tf32_rna(r1 - a1[u]);
+        }
+        float *dst = pack + (size_t(blockIdx.z) * m + b0 + r) * kPackRow + 4 * q;
+        *reinterpret_cast<float4 *>(dst) = p0;
+        *reinterpret_cast<float4 *>(dst + 128) = p1;
+        *reinterpret_cast<float4 *>(dst + 256) = p2;
+    }
+}
+
 // -------------------------------------------------------------- update --
 // Rows [r_lo, r_hi) x columns [c_lo, c_hi) of the trailing block after the
 // panels [k0, k0 + K) (relative to r0 = k0 + K), in 128 x 128 tiles; K =
@@ -342,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ------------------------------------------------ MMA issuer
         if (lane == 0) {
             uint32_t g = 0;  // stages consumed
-            uint32_t u = 0;  // accumulator rounds: one per (tile, K chunk)
+            uint32_t u = 0;  // tiles issued (accumulator pair u & 1)
             bool ok = true;
             for (uint32_t i = 0; ok; ++i) {
                 const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
@@ -353,15 +417,22 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t t = tile_id[slot];
                 mbar_arrive(&tile_empty[slot]);
                 if (t >= total) break;
-                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g, ++u) {
-                    const uint32_t a = u & 1, aph = (u >> 1) & 1;
+                // the tile's accumulator pair: free once the epilogue has read
+                // the tile two before this one
+                const uint32_t a = u & 1, aph = (u >> 1) & 1;
+                ++u;
+                if (!mbar_wait(&acc_empty[a], aph ^ 1, spin_limit)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t d_big = tmem + a * 2 * kTile, d_small = d_big + kTile;
+                for (uint32_t kc = 0; kc < nchunks; ++kc, ++g) {
                     const uint32_t s = g % kStages, ph = (g / kStages) & 1;
-                    if (!mbar_wait(&acc_empty[a], aph ^ 1, spin_limit) || !mbar_wait(&full[s], ph, spin_limit)) {
+                    if (!mbar_wait(&full[s], ph, spin_limit)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t d_big = tmem + a * 2 * kTile, d_small = d_big + kTile;
                     const uint32_t base = smem_addr(smem + s * kStageBytes);
 #pragma unroll
                     for (uint32_t k8 = 0; k8 < kChunk / 8; ++k8) {
@@ -372,7 +443,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                             A[p] = kmajor_sw128_desc(base + p * kOpBytes + off);
                             B[p] = kmajor_sw128_desc(base + (kParts + p) * kOpBytes + off);
                         }
-                        const uint32_t acc = k8 != 0;
+                        const uint32_t acc = (kc | k8) != 0;
                         tc_mma_tf32(d_small, A[2], B[0], acc);  // 2^-22 terms first
                         tc_mma_tf32(d_small, A[1], B[1], 1);
                         tc_mma_tf32(d_small, A[0], B[2], 1);
@@ -381,8 +452,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                         tc_mma_tf32(d_big, A[0], B[0], acc);
                     }
                     tc_commit(&empty[s]);
-                    tc_commit(&acc_full[a]);
                 }
+                if (!ok) break;
+                tc_commit(&acc_full[a]);
             }
             if (!ok) atomicOr(status, DEV_TIMEOUT);
             tc_commit(done);
@@ -405,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
         }
-        uint32_t u = 0;  // accumulator rounds, as the MMA issuer counts them
+        uint32_t u = 0;  // tiles taken, as the MMA issuer counts them
         for (uint32_t i = 0;; ++i) {
             const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
             if (!__all_sync(0xffffffffu, mbar_wait(&tile_full[slot], sph, spin_limit))) {
@@ -437,35 +509,30 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
                     c[cc][jj] = ok ? ld_cg(val + o + grow) : 0.0f;
                 }
-            // the chunks' partial sums, subtracted in K order in FP32
-            bool ok = true;
-            for (uint32_t kc = 0; kc < nchunks; ++kc, ++u) {
-                const uint32_t a = u & 1, aph = (u >> 1) & 1;
-                // warp-uniform: the tcgen05.ld below needs the whole warp
-                if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[a], aph, spin_limit))) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t lane_base = tmem + ((q * 32) << 16) + a * 2 * kTile;
-#pragma unroll
-                for (int cc = 0; cc < 4; ++cc) {
-                    float acc[32];
-                    tc_ld32(lane_base + cc * 32, acc);  // big
-#pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
-                    tc_ld32(lane_base + kTile + cc * 32, acc);  // small
-#pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&acc_empty[a]);
-            }
-            if (!ok) {
+            // the tile's two sums, subtracted in FP32: c := (c - big) - small
+            const uint32_t a = u & 1, aph = (u >> 1) & 1;
+            ++u;
+            // warp-uniform: the tcgen05.ld below needs the whole warp
+            if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[a], aph, spin_limit))) {
                 if (lane == 0) atomicOr(status, DEV_TIMEOUT);
                 break;
             }
+            tc_fence_after();
+            const uint32_t lane_base = tmem + ((q * 32) << 16) + a * 2 * kTile;
+#pragma unroll
+            for (int cc = 0; cc < 4; ++cc) {
+                float acc[32];
+                tc_ld32(lane_base + cc * 32, acc);  // big
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
+                tc_ld32(lane_base + kTile + cc * 32, acc);  // small
+#pragma unroll
+                for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
+            }
+            // the pair takes the tile after next while this one is stored
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[a]);
 #pragma unroll
             for (int cc = 0; cc < 4; ++cc)
 #pragma unroll
@@ -524,31 +591,67 @@ cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count,
     return cudaGetLastError();
 }
 
-cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
-                                   uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
-                                   const float *diag_scratch, DenseRegion reg, uint32_t *status,
-                                   uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter, cudaStream_t st) {
+namespace {
+// Rows [r_lo, r_hi) x columns [c_lo, c_hi) of the block from row and column
+// r0 on, K = 32 * nchunks.
+cudaError_t launch_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride, uint32_t count,
+                      const uint32_t *doff, uint32_t m, uint32_t r0, uint32_t nchunks, const float *diag_scratch,
+                      DenseRegion reg, uint32_t *status, uint32_t spin_limit, uint32_t num_sms,
+                      uint32_t *tile_counter, cudaStream_t st) {
     static PerDeviceOnce attr;
     cudaError_t e = attr.run([] {
         return cudaFuncSetAttribute(k_dense_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSmemBytes));
     });
     if (e != cudaSuccess) return e;
-    const uint32_t r0 = k0 + kb;
     const uint32_t rows = reg.r_hi > reg.r_lo ? reg.r_hi - reg.r_lo : 0;
     const uint32_t cols = reg.c_hi > reg.c_lo ? reg.c_hi - reg.c_lo : 0;
     const uint32_t tiles_r = (rows + kTile - 1) / kTile, tiles_c = (cols + kTile - 1) / kTile;
     const uint64_t total = uint64_t(tiles_r) * tiles_c * count;
     if (total == 0 && !reg.writeback) return cudaSuccess;
-    if (r0 > m || total > 0xFFFFFFFFull) return cudaErrorInvalidValue;
+    if (r0 > m || total > 0xFFFFFFFFull || nchunks == 0 || nchunks * kChunk > 128) return cudaErrorInvalidValue;
     uint32_t grid = uint32_t(std::min<uint64_t>(std::max<uint64_t>(total, 1), num_sms));
     if (reg.writeback) grid = std::max<uint32_t>(grid, std::min<uint32_t>(count, num_sms));
-    const uint32_t nchunks = (kb + kChunk - 1) / kChunk;
     e = cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     k_dense_update_tc<<<grid, kThreads, kSmemBytes, st>>>(mapA, mapB, val, stride, doff, m, r0, nchunks, reg,
                                                           tiles_r, tiles_c, count, diag_scratch, status, spin_limit,
                                                           tile_counter);
     return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
+                                   uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
+                                   const float *diag_scratch, DenseRegion reg, uint32_t *status,
+                                   uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter, cudaStream_t st) {
+    return launch_tc(mapA, mapB, val, stride, count, doff, m, k0 + kb, (kb + kChunk - 1) / kChunk, diag_scratch, reg,
+                     status, spin_limit, num_sms, tile_counter, st);
+}
+
+cudaError_t launch_couple_pack(const DevPattern &P, const float *val, uint64_t stride, uint32_t count, uint32_t t,
+                               uint32_t m, uint32_t ncols, uint32_t slot0, const uint32_t *lstart,
+                               const uint32_t *ustart, float *packA, float *packB, cudaStream_t st) {
+    if (m == 0 || ncols == 0) return cudaSuccess;
+    if (ncols > uint32_t(kTile)) return cudaErrorInvalidValue;
+    static PerDeviceOnce attr;
+    cudaError_t e = attr.run([] {
+        return cudaFuncSetAttribute(k_couple_pack, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kCoupleSmem));
+    });
+    if (e != cudaSuccess) return e;
+    const uint32_t nblk = (m + kTile - 1) / kTile;
+    k_couple_pack<<<dim3(2 * nblk, 1, count), kTile, kCoupleSmem, st>>>(P.ridx, P.cidx, P.cpos, val, stride, t, m,
+                                                                      ncols, slot0, lstart, ustart, nblk, packA,
+                                                                      packB);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_couple_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
+                                    uint32_t count, const uint32_t *doff, uint32_t m, uint32_t ncols,
+                                    uint32_t *status, uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter,
+                                    cudaStream_t st) {
+    const DenseRegion reg{0, m, 0, m, 0, 0};
+    return launch_tc(mapA, mapB, val, stride, count, doff, m, 0, (ncols + kChunk - 1) / kChunk, nullptr, reg, status,
+                     spin_limit, num_sms, tile_counter, st);
 }
 
 }  // namespace glu

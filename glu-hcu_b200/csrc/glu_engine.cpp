@@ -99,12 +99,12 @@ static cudaError_t upload(DevBuf &d, const std::vector<T> &h) {
 // Kernel kinds of glu_factor for the optional per-kernel profile.
 enum KernelKind {
     KK_PERT = 0, KK_LEVEL, KK_CHAIN, KK_SCALE, KK_DGATHER, KK_PANEL, KK_UPDATE, KK_DSCATTER, KK_CHECK,
-    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE, KK_PACK, KK_UPDATE_TC, KK_DIAG_INV
+    KK_SN_DIAG, KK_SN_PANEL, KK_SN_UPDATE, KK_PACK, KK_UPDATE_TC, KK_DIAG_INV, KK_COUPLE_PACK
 };
 static const char *const kKindNames[GLU_KERNEL_KINDS] = {
     "k_colsum+k_pert_finish", "k_factor_level", "k_factor_chain", "k_scale_level", "k_dense_gather",
     "k_dense_panel", "k_dense_update", "k_dense_scatter", "k_check_pivots", "k_sn_diag", "k_sn_panel",
-    "k_sn_update", "k_dense_pack", "k_dense_update_tc", "k_dense_diag_inv"};
+    "k_sn_update", "k_dense_pack", "k_dense_update_tc", "k_dense_diag_inv", "k_couple_pack"};
 
 // Events around every launch of one glu_factor call, when enabled.
 struct KernelProfiler {
@@ -165,6 +165,9 @@ struct Step {
     int kind;
     uint32_t l0, l1;  // sparse levels [l0, l1)
 };
+struct CoupleGroup {
+    uint32_t c0, c1;  // deferred columns [c0, c1) (slots)
+};
 
 }  // namespace glu
 
@@ -203,6 +206,13 @@ struct glu_handle_s {
     DevBuf d_sn_meta, d_sn_dmap, d_sn_dsmall, d_sn_pmap, d_sn_umap, d_sn_psmall, d_sn_usmall, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
+    // deferred coupling of the sparse part into the dense tail: per supernode
+    // its cut, per deferred column and 128-wide tail block the CSC range of
+    // its tail rows and the CSR range of its tail columns there, the groups
+    // of up to 128 columns
+    DevBuf d_sn_cut, d_couple_lstart, d_couple_ustart;
+    std::vector<CoupleGroup> couple_groups;
+    uint32_t couple_cols = 0;
     DevBuf d_ss_map[2], d_ss_meta[2], d_ss_small[2];  // supernodal L and U sweeps
     DevBuf d_ss_woff[2], d_ss_widx[2], d_ss_roff[2], d_ss_ridx[2], d_ss_indeg[2];  // their fused form
     DevBuf d_sweep_done;  // per value set and supernode: releases received (fused sweeps)
@@ -320,6 +330,10 @@ constexpr double kDenseRate = 30e12, kDenseRateTc = 120e12, kPanelLatency = 20e-
 constexpr uint32_t kLookaheadMin = 3072;
 // Default width from which trailing blocks update on the tensor cores.
 constexpr uint32_t kDenseTcMin = 1024;
+// Cost of one deferred coupling product (up to 128 columns over the whole
+// m x m dense block), in scattered supernode-update entries per entry of the
+// block.
+constexpr double kCoupleGroupCost = 1.0;
 constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
 
 uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
@@ -458,6 +472,8 @@ Status build_sn_plan(glu_handle_s *h) {
     h->use_sn = width > 0 && t > 0;
     h->nsn = 0;
     h->sn_levels.clear();
+    h->couple_groups.clear();
+    h->couple_cols = 0;
     h->stats.sn_update_flops = h->stats.sn_update_bytes = h->stats.sn_panel_bytes = 0;
     h->S.sn[0] = SnSweepPlan{};
     h->S.sn[1] = SnSweepPlan{};
@@ -509,6 +525,74 @@ Status build_sn_plan(glu_handle_s *h) {
         std::vector<uint32_t> cur(lcount.begin(), lcount.end() - 1);
         for (uint32_t q = 0; q < ns; ++q) order[cur[lev[q]]++] = q;
     }
+    // Deferred coupling: supernode q's update of the dense tail is the corner
+    // of its L21 rows >= t (a suffix of a rows) by its targets >= t (a suffix
+    // of b).  When the tail updates on the tensor cores, the supernodes with
+    // the largest corners per column leave theirs to tensor-core products
+    // after the sparse part, up to 128 columns each.  A product costs about
+    // kCoupleGroupCost m^2 scattered entry updates (the whole block's C read
+    // and written, the MMAs), divided by tune.defer_tail; the prefix of
+    // supernodes, by corner area per column, that saves most is taken.
+    std::vector<uint32_t> ca(ns, 0), cb(ns, 0);
+    std::vector<uint8_t> deferred(ns, 0);
+    const bool tc_tail = h->m && h->tune.dense_tc_min && h->m >= h->tune.dense_tc_min;
+    if (tc_tail && h->tune.defer_tail) {
+        std::vector<std::pair<double, uint32_t>> cand;
+        for (uint32_t q = 0; q < ns; ++q) {
+            const uint32_t w = first[q + 1] - first[q], last = first[q + 1] - 1;
+            const uint32_t *r0 = s.sym_r_idx.data() + s.l_col_ptr[last] + 1, *r1 = s.sym_r_idx.data() + s.sym_c_ptr[last + 1];
+            const uint32_t *c0 = s.csr_c_idx.data() + s.csr_diag_ptr[last] + 1, *c1 = s.csr_c_idx.data() + s.csr_r_ptr[last + 1];
+            ca[q] = uint32_t(r1 - std::lower_bound(r0, r1, t));
+            cb[q] = uint32_t(c1 - std::lower_bound(c0, c1, t));
+            const bool small = h->tune.sn_small && w <= kSnSmallWidth && (r1 - r0) <= 32 && (c1 - c0) <= 32;
+            if (!small && ca[q] && cb[q]) cand.push_back({double(ca[q]) * cb[q] / w, q});
+        }
+        std::sort(cand.begin(), cand.end(), [](const auto &x, const auto &y) {
+            return x.first != y.first ? x.first > y.first : x.second < y.second;
+        });
+        const double group_cost = kCoupleGroupCost * double(h->m) * h->m / h->tune.defer_tail;
+        double saved = 0, best = 0;
+        uint64_t cols = 0;
+        size_t take = 0;
+        for (size_t c = 0; c < cand.size(); ++c) {
+            const uint32_t q = cand[c].second;
+            cols += first[q + 1] - first[q];
+            saved += double(ca[q]) * cb[q];
+            const double gain = saved - double((cols + kTcTile - 1) / kTcTile) * group_cost;
+            if (gain > best) {
+                best = gain;
+                take = c + 1;
+            }
+        }
+        for (size_t c = 0; c < take; ++c) deferred[cand[c].second] = 1;
+        if (take) {
+            // deferred columns ascending; per slot and 128-wide tail block the
+            // CSC positions of its tail rows and the CSR positions of its tail
+            // columns that fall in the block
+            std::vector<uint32_t> kcols;
+            for (uint32_t q = 0; q < ns; ++q)
+                if (deferred[q])
+                    for (uint32_t k = first[q]; k < first[q + 1]; ++k) kcols.push_back(k);
+            const uint32_t nblk = (h->m + kTcTile - 1) / kTcTile;
+            std::vector<uint32_t> lstart(kcols.size() * (nblk + 1)), ustart(kcols.size() * (nblk + 1));
+            for (size_t g = 0; g < kcols.size(); ++g) {
+                const uint32_t k = kcols[g];
+                const uint32_t *r0 = s.sym_r_idx.data() + s.sym_c_ptr[k], *r1 = s.sym_r_idx.data() + s.sym_c_ptr[k + 1];
+                const uint32_t *c0 = s.csr_c_idx.data() + s.csr_r_ptr[k], *c1 = s.csr_c_idx.data() + s.csr_r_ptr[k + 1];
+                for (uint32_t b = 0; b <= nblk; ++b) {
+                    const uint32_t key = t + std::min<uint32_t>(b * kTcTile, h->m);
+                    lstart[g * (nblk + 1) + b] = uint32_t(std::lower_bound(r0, r1, key) - s.sym_r_idx.data());
+                    ustart[g * (nblk + 1) + b] = uint32_t(std::lower_bound(c0, c1, key) - s.csr_c_idx.data());
+                }
+            }
+            for (uint32_t c0 = 0; c0 < kcols.size(); c0 += kTcTile)
+                h->couple_groups.push_back(CoupleGroup{c0, std::min<uint32_t>(uint32_t(kcols.size()), c0 + kTcTile)});
+            h->couple_cols = uint32_t(kcols.size());
+            GLU_CUDA(upload(h->d_couple_lstart, lstart), "upload coupling plan");
+            GLU_CUDA(upload(h->d_couple_ustart, ustart), "upload coupling plan");
+        }
+    }
+    std::vector<uint2> cut(ns);
     std::vector<uint4> meta(ns);
     std::vector<uint2> pmap, umap;
     std::vector<uint32_t> psmall, usmall, dsmall, tgt(size_t(ns) + 1, 0);
@@ -544,14 +628,21 @@ Status build_sn_plan(glu_handle_s *h) {
                 for (uint64_t bb = 0; bb < pb; ++bb) pmap.push_back(make_uint2(i, uint32_t(bb)));
                 panel_w = std::max(panel_w, w);
             }
+            // rows [row_cut, m) x targets [tgt_cut, nt): the deferred corner
+            const uint64_t row_cut = deferred[q] ? m - ca[q] : m, tgt_cut = deferred[q] ? nt - cb[q] : nt;
+            cut[i] = make_uint2(uint32_t(row_cut), uint32_t(tgt_cut));
+            const uint64_t nrt = (m + UT - 1) / UT;
             if (tiles && small && m * nt <= 256)
                 usmall.push_back(i);
             else
-                for (uint64_t bb = 0; bb < tiles; ++bb) umap.push_back(make_uint2(i, uint32_t(bb)));
+                for (uint64_t bb = 0; bb < tiles; ++bb)
+                    if ((bb % nrt) * UT < row_cut || (bb / nrt) * UT < tgt_cut)
+                        umap.push_back(make_uint2(i, uint32_t(bb)));
             tgt[i + 1] = tgt[i] + uint32_t(nt);
             pos_off[i + 1] = pos_off[i] + m * nt;
-            upd_flops += 2.0 * double(m) * w * nt;
-            upd_bytes += 4.0 * (double(m) * w + double(w) * nt) + 8.0 * double(m) * nt;
+            const double kept = double(m) * nt - double(m - row_cut) * (nt - tgt_cut);
+            upd_flops += 2.0 * kept * w;
+            upd_bytes += 4.0 * (double(m) * w + double(w) * nt) + 8.0 * kept;
             pan_bytes += 8.0 * (double(m) * w + double(w) * nt) + (w >= 2 ? 8.0 * w * w : 0.0);
         }
         for (size_t g = ps0; g < psmall.size(); g += kSnPanelThreads / 32)
@@ -576,11 +667,13 @@ Status build_sn_plan(glu_handle_s *h) {
     GLU_CUDA(upload(h->d_sn_usmall, usmall), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_tgt_off, tgt), "upload supernodes");
     GLU_CUDA(upload(h->d_sn_pos_off, pos_off), "upload supernodes");
+    if (h->couple_cols) GLU_CUDA(upload(h->d_sn_cut, cut), "upload coupling plan");
     GLU_CUDA(h->d_sn_tgt.alloc(sizeof(uint4) * std::max<uint32_t>(tgt[ns], 1)), "allocate supernode targets");
     h->SN = SnPlanDev{h->d_sn_meta.as<uint4>(),      h->d_sn_dmap.as<uint2>(),  h->d_sn_dsmall.as<uint32_t>(),
                       h->d_sn_pmap.as<uint2>(),      h->d_sn_umap.as<uint2>(),
                       h->d_sn_psmall.as<uint32_t>(), h->d_sn_usmall.as<uint32_t>(), h->d_sn_tgt_off.as<uint32_t>(),
                       h->d_sn_tgt.as<uint4>(),       nullptr,                    h->d_sn_pos_off.as<uint64_t>()};
+    if (h->couple_cols) h->SN.cut = h->d_sn_cut.as<uint2>();
     GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
     GLU_CUDA(cudaDeviceSynchronize(), "supernode targets");
     // Position table of the update scatter, when it fits in a quarter of the
@@ -912,6 +1005,8 @@ Status build_plan(glu_handle_s *h) {
     h->stats.dense_tail = m;
     h->stats.factor_flops = flops;
     h->stats.supernodes = h->nsn;
+    h->stats.couple_columns = h->couple_cols;
+    h->stats.couple_groups = uint32_t(h->couple_groups.size());
     h->stats.sn_levels = uint32_t(h->sn_levels.size());
     uint64_t launches = 2;
     if (h->use_sn) {
@@ -919,7 +1014,7 @@ Status build_plan(glu_handle_s *h) {
     } else {
         launches += h->steps.size() + (NL ? 1 : 0);
     }
-    if (m) launches += 2 * ((m + kDenseNB - 1) / kDenseNB) + (h->dense_buffer ? 2 : 0);
+    if (m) launches += 2 * ((m + kDenseNB - 1) / kDenseNB) + (h->dense_buffer ? 2 : 0) + 2 * h->couple_groups.size();
     h->stats.factor_launches = launches;
     return GLU_OK;
 }
@@ -952,7 +1047,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->batch = batch;
     h->pat = std::move(s);
     h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 1u,
-                         0u};
+                         0u, 1u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -1562,10 +1657,6 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     float *dscr = h->d_diag_scratch.as<float>();
     cudaStream_t ps = lookahead ? h->aux : st;  // panels and strips
     bool rest_pending = false;
-    if (lookahead) {
-        GLU_CUDA(cudaEventRecord(h->ev_fork, st), "event");
-        GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_fork, 0), "stream wait");
-    }
     const uint32_t nb = kDenseNB;
     // tensor-core updates for wide trailing blocks; their operand packs are
     // allocated once per handle
@@ -1581,6 +1672,31 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     }
     uint32_t *dstatus = h->d_status.as<uint32_t>();
     double upd_bytes = 0, upd_flops = 0;
+    // The sparse columns' deferred updates of the block (the plan has them
+    // only when the block updates on the tensor cores): per group of up to 128
+    // columns, their tail rows of L and tail columns of U into the packs, then
+    // A22 -= L U over the whole block.
+    if (tc && !h->couple_groups.empty()) {
+        const double mm = h->m;
+        for (const CoupleGroup &gr : h->couple_groups) {
+            const uint32_t nc = gr.c1 - gr.c0;
+            GLU_LAUNCH(KK_COUPLE_PACK,
+                       launch_couple_pack(h->P, val, stride, count, h->t, h->m, nc, gr.c0,
+                                          h->d_couple_lstart.as<uint32_t>(), h->d_couple_ustart.as<uint32_t>(),
+                                          h->d_packA.as<float>(), h->d_packB.as<float>(), st),
+                       "factor (coupling pack)");
+            GLU_LAUNCH(KK_UPDATE_TC,
+                       launch_couple_update_tc(h->map_packA, h->map_packB, dbase, dstride, count, doff, h->m, nc,
+                                               dstatus, h->spin_limit, h->num_sms, h->d_tc_counter.as<uint32_t>(), st),
+                       "factor (coupling update)");
+            upd_bytes += double(count) * (8.0 * mm * mm + 8.0 * nc * mm);
+            upd_flops += double(count) * 2.0 * nc * mm * mm;
+        }
+    }
+    if (lookahead) {
+        GLU_CUDA(cudaEventRecord(h->ev_fork, st), "event");
+        GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_fork, 0), "stream wait");
+    }
     // A region goes to the tensor cores when its area over all value sets
     // reaches two 128 x 128 tiles per SM, or dense_tc_min^2 entries if less;
     // thinner ones (the look-ahead strips, the last small updates) stay on the

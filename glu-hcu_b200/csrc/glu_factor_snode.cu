@@ -416,7 +416,10 @@ __global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, S
 // supernodes accumulate with atomics (numeric.cu:82); a single supernode
 // updates each entry from one thread: C is loaded, the K products are applied
 // in column order, C is stored.  Target positions come from the precomputed
-// table S.pos when present, else from a search in column j's rows.
+// table S.pos when present, else from a search in column j's rows.  A
+// supernode whose update of the dense tail is deferred (S.cut) skips the
+// entries of that corner; the update map holds none of its tiles that lie
+// wholly inside it.
 __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S, float *val_base, uint64_t stride,
                                                       uint32_t b0, uint32_t atomic, uint32_t count, uint32_t zpb) {
     __shared__ __align__(16) float sL[kSnMaxWidth][kTLd];
@@ -505,6 +508,14 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
                 pos[a][bb] = q;
             }
         }
+    }
+    if (S.cut) {  // the deferred corner (tail rows x tail targets) is left out
+        const uint2 cu = __ldg(S.cut + i);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb)
+                if (r0 + tr * 4 + a >= cu.x && c0 + tc * 4 + bb >= cu.y) pos[a][bb] = 0xffffffffu;
     }
     for (uint32_t z = z0; z < z1; ++z) {
     float *val = val_base + z * stride;

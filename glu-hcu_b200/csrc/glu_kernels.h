@@ -68,6 +68,11 @@ struct SnPlanDev {
     const uint32_t *tail_start = nullptr;
     uint32_t t = 0;
     uint32_t tail_full = 0;
+    // Per supernode (level order), when any defers its update of the dense
+    // tail: {first L21 row, first target} of the deferred corner (rows and
+    // targets in the tail); updates there are skipped.  {m, nt} for the
+    // others.  nullptr: none deferred.
+    const uint2 *cut = nullptr;
 };
 
 // Blocks [b0, b0 + blocks) of one level's diagonal-block, panel or update
@@ -120,6 +125,25 @@ cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &m
                                    uint32_t count, const uint32_t *doff, uint32_t m, uint32_t k0, uint32_t kb,
                                    const float *diag_scratch, DenseRegion reg, uint32_t *status,
                                    uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter, cudaStream_t st);
+// The deferred coupling of the sparse part into the trailing block: sparse
+// columns whose update of the block is large skip it in the supernodal
+// updates (their supernode's cut), and after the sparse part the block takes
+// A22 -= L(tail, K) U(K, tail) for the deferred columns K, in groups of up to
+// 128 (slots slot0 .. slot0 + ncols - 1 of all deferred columns).
+// couple_pack writes one group's operands into the packs: for slot g and
+// 128-wide tail block b, lstart[g][b] .. lstart[g][b + 1] are the CSC
+// positions of column k_g's rows in tail rows [128 b, 128 b + 128), and
+// ustart[g][b] .. ustart[g][b + 1] the CSR positions of row k_g's entries in
+// tail columns [128 b, 128 b + 128) (nblk + 1 entries per slot, nblk = the
+// tail's 128-blocks).  couple_update_tc is the tensor-core update of the whole
+// block from those packs.
+cudaError_t launch_couple_pack(const DevPattern &P, const float *val, uint64_t stride, uint32_t count, uint32_t t,
+                               uint32_t m, uint32_t ncols, uint32_t slot0, const uint32_t *lstart,
+                               const uint32_t *ustart, float *packA, float *packB, cudaStream_t st);
+cudaError_t launch_couple_update_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *val, uint64_t stride,
+                                    uint32_t count, const uint32_t *doff, uint32_t m, uint32_t ncols,
+                                    uint32_t *status, uint32_t spin_limit, uint32_t num_sms, uint32_t *tile_counter,
+                                    cudaStream_t st);
 // A trailing block that is dense but not completely filled is factored in a
 // separate m x m column-major buffer: gather copies the block's pattern
 // entries of the CSC values into the (zeroed) buffer, scatter copies the

@@ -206,7 +206,8 @@ static cudaError_t run_sweep(const DevPattern &P, const SolvePlanDev &S, const f
 //   kMode 2: T = U^T (lower,           T(i,c) = val[doff[i] + c])
 //   kMode 3: T = L^T (unit upper,      T(i,c) = val[doff[i] + c])
 // Row blocks of 64 are claimed in solve order (ascending for lower, descending
-// for upper); flags[b] = 1 once block b is solved.  The diagonal block's
+// for upper), interleaved over the value sets; flags[b] = 1 once block b of
+// a set is solved.  The diagonal block's
 // solve is a product with its inverse (dinv, computed once per factorization
 // by k_dense_diag_inv), so the step between two blocks of the chain is a
 // parallel 64 x 64 mat-vec instead of 64 dependent substitution steps.
@@ -266,15 +267,18 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     __shared__ uint32_t s_blk;
     const uint32_t tid = threadIdx.x;
     const uint32_t nb = (m + kRB - 1) / kRB;
-    // value set blockIdx.z: its factors, right-hand sides, block flags, ticket
-    val += blockIdx.z * dstride;
-    y += blockIdx.z * ystride;
-    flags += size_t(blockIdx.z) * nb;
-    ticket += blockIdx.z;
+    // One ticket counter for the launch, handed out block-row-major over the
+    // value sets (ticket = block * count + set): every set's chain advances
+    // at once, and a block waits only on blocks of smaller tickets, which
+    // are running or done.
     if (tid == 0) s_blk = atomicAdd(ticket, 1u) + ticket_base;
     __syncthreads();
-    const uint32_t tk = s_blk;
-    if (tk >= nb) return;
+    const uint32_t count = gridDim.z, tg = s_blk;
+    if (tg >= nb * count) return;
+    const uint32_t z = tg % count, tk = tg / count;
+    val += z * dstride;
+    y += z * ystride;
+    flags += size_t(z) * nb;
     const uint32_t b = kLower ? tk : nb - 1 - tk;
     const uint32_t rb0 = b * kRB, rb1 = min(rb0 + kRB, m);
     const uint32_t rows = rb1 - rb0;
@@ -285,33 +289,37 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     // issued first (row-major; transposed for the transposed sweeps)
     constexpr int kTilePer = kRB * kRB / 256;
     float dv[kTilePer];
-    const float *inv = dinv + ((size_t(blockIdx.z) * nb + b) * 2 + kWhich) * kRB * kRB;
+    const float *inv = dinv + ((size_t(z) * nb + b) * 2 + kWhich) * kRB * kRB;
 #pragma unroll
     for (int qq = 0; qq < kTilePer; ++qq) dv[qq] = __ldg(inv + tid + qq * 256);
+    // tile T(rb0.., block s in solve order): independent of x
+    auto load_tile = [&](uint32_t s, float (&tv)[kTilePer]) {
+        const uint32_t c = kLower ? s : nb - 1 - s;
+        const uint32_t cb0 = c * kRB, cb1 = min(cb0 + kRB, m);
+#pragma unroll
+        for (int qq = 0; qq < kTilePer; ++qq) {
+            const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;  // coalesced along bb
+            const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+            tv[qq] = (rb0 + i < rb1 && cb0 + cc < cb1) ? T(rb0 + i, cb0 + cc) : 0.0f;
+        }
+    };
     for (uint32_t rc0 = 0; rc0 < nrhs; rc0 += kRHSChunk) {
         const uint32_t nr = min(uint32_t(kRHSChunk), nrhs - rc0);
         const uint32_t row = tid & (kRB - 1), q = tid / kRB;  // 4 quarters of 16 columns
         float acc[kRHSChunk] = {0.f, 0.f, 0.f, 0.f};
-        // contributions of the finished blocks, in solve order
+        // contributions of the finished blocks, in solve order; the next
+        // block's tile is in flight while this one waits and computes
+        float tv[kTilePer], tn[kTilePer];
+        if (tk > 0) load_tile(0, tv);
         for (uint32_t s = 0; s < tk; ++s) {
             const uint32_t c = kLower ? s : nb - 1 - s;
             const uint32_t cb0 = c * kRB, cb1 = min(cb0 + kRB, m);
-            // stage tile T(rb0.., cb0..): it does not depend on x, so it is
-            // loaded before waiting for block c, all loads of a thread in flight
-            {
-                float tv[kTilePer];
+            if (s + 1 < tk) load_tile(s + 1, tn);
 #pragma unroll
-                for (int qq = 0; qq < kTilePer; ++qq) {
-                    const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;  // coalesced along bb
-                    const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
-                    tv[qq] = (rb0 + i < rb1 && cb0 + cc < cb1) ? T(rb0 + i, cb0 + cc) : 0.0f;
-                }
-#pragma unroll
-                for (int qq = 0; qq < kTilePer; ++qq) {
-                    const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
-                    const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
-                    tile[i][cc] = tv[qq];
-                }
+            for (int qq = 0; qq < kTilePer; ++qq) {
+                const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
+                const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
+                tile[i][cc] = tv[qq];
             }
             if (tid == 0) wait_count(flags + c, 1u, status, spin_limit);
             __syncthreads();
@@ -324,11 +332,13 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
             __syncthreads();
 #pragma unroll 4
             for (uint32_t cc = q * 16; cc < q * 16 + 16; ++cc) {
-                float tv = tile[row][cc];
+                float tv2 = tile[row][cc];
 #pragma unroll
-                for (int r = 0; r < kRHSChunk; ++r) acc[r] = fmaf(tv, xs[cc][r], acc[r]);
+                for (int r = 0; r < kRHSChunk; ++r) acc[r] = fmaf(tv2, xs[cc][r], acc[r]);
             }
             __syncthreads();
+#pragma unroll
+            for (int qq = 0; qq < kTilePer; ++qq) tv[qq] = tn[qq];
         }
 #pragma unroll
         for (int r = 0; r < kRHSChunk; ++r) part[q][row][r] = acc[r];

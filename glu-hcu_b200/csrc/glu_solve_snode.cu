@@ -114,25 +114,32 @@ __device__ __forceinline__ void sn_sweep_u_small(const DevPattern &P, const SnSw
         if (ev && xe != 0.0f) atomicAdd(yq + tg, -__fmul_rn(ue, xe));
     }
 }
-// Fused sweeps: the block's item from a ticket in dispatch order, and a
-// wait (thread 0, bounded) until every supernode it solves has received all
-// its releases.  Returns the map index, or UINT32_MAX when the ticket is past
-// the end.  Per-level launches use b0 + blockIdx.x instead.
-__device__ __forceinline__ uint32_t sweep_block(const SnSweepPlan &W, uint32_t b0, const uint32_t *done,
-                                                uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
-    if (!done) return b0 + blockIdx.x;
-    __shared__ uint32_t s_blk;
+// Fused sweeps: the block's item and value set from one ticket counter of the
+// launch, handed out item-major over the value sets (ticket = item * count +
+// set, so every set's sweep advances at once), and a wait (thread 0, bounded)
+// until every supernode it solves has received all its releases; a block
+// waits only on items of smaller tickets.  Returns {map index, value set},
+// the index UINT32_MAX when the ticket is past the end.  Per-level launches
+// use {b0 + blockIdx.x, blockIdx.z} instead.
+__device__ __forceinline__ uint2 sweep_block(const SnSweepPlan &W, uint32_t b0, const uint32_t *done,
+                                             uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
+    if (!done) return make_uint2(b0 + blockIdx.x, blockIdx.z);
+    __shared__ uint32_t s_blk, s_z;
     if (threadIdx.x == 0) {
-        uint32_t k = atomicAdd(ticket + blockIdx.z, 1u);
-        if (k < W.nblocks)
-            for (uint32_t e = W.wait_off[k]; e < W.wait_off[k + 1]; ++e) {
+        const uint32_t k = atomicAdd(ticket, 1u);
+        const uint32_t blk = k / gridDim.z, z = k % gridDim.z;
+        if (blk < W.nblocks) {
+            const uint32_t *dz = done + size_t(z) * W.ns;
+            for (uint32_t e = W.wait_off[blk]; e < W.wait_off[blk + 1]; ++e) {
                 const uint32_t q = W.wait_idx[e];
-                wait_count(done + q, W.indeg[q], status, spin_limit);
+                wait_count(dz + q, W.indeg[q], status, spin_limit);
             }
-        s_blk = k;
+        }
+        s_blk = blk;
+        s_z = z;
     }
     __syncthreads();
-    return s_blk < W.nblocks ? s_blk : UINT32_MAX;
+    return make_uint2(s_blk < W.nblocks ? s_blk : UINT32_MAX, s_z);
 }
 
 // After the block's scatter: one release for every supernode it updated (its
@@ -151,11 +158,12 @@ __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
                                                     uint64_t vstride, uint64_t ystride, uint32_t *done,
                                                     uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
-    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
-    y += blockIdx.z * ystride;
-    xo += blockIdx.z * ystride;
-    if (done) done += size_t(blockIdx.z) * W.ns;
-    const uint32_t blk = sweep_block(W, b0, done, ticket, status, spin_limit);
+    const uint2 bz = sweep_block(W, b0, done, ticket, status, spin_limit);
+    const uint32_t blk = bz.x;
+    val += bz.y * vstride;  // value set bz.y, its right-hand sides
+    y += bz.y * ystride;
+    xo += bz.y * ystride;
+    if (done) done += size_t(bz.y) * W.ns;
     if (blk == UINT32_MAX) return;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];
@@ -234,11 +242,12 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
                                                     uint64_t vstride, uint64_t ystride, uint32_t *done,
                                                     uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
-    val += blockIdx.z * vstride;  // value set blockIdx.z, its right-hand sides
-    y += blockIdx.z * ystride;
-    xo += blockIdx.z * ystride;
-    if (done) done += size_t(blockIdx.z) * W.ns;
-    const uint32_t blk = sweep_block(W, b0, done, ticket, status, spin_limit);
+    const uint2 bz = sweep_block(W, b0, done, ticket, status, spin_limit);
+    const uint32_t blk = bz.x;
+    val += bz.y * vstride;  // value set bz.y, its right-hand sides
+    y += bz.y * ystride;
+    xo += bz.y * ystride;
+    if (done) done += size_t(bz.y) * W.ns;
     if (blk == UINT32_MAX) return;
     __shared__ float sT[kSnMaxWidth * kLD];
     __shared__ float xs[kSnMaxWidth];

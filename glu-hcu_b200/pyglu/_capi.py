@@ -41,7 +41,7 @@ ENGINE_SYMBOLS = [
     "glu_kernel_kind_name", "glu_measure_fp32_peak", "glu_set_wait_limit", "glu_debug_inject",
     "glu_factor_many", "glu_solve_refined_many",
 ]
-GLU_KERNEL_KINDS = 15
+GLU_KERNEL_KINDS = 16
 PRE_SYMBOLS = [
     "glu_pre_analyze", "glu_pre_n", "glu_pre_nnz", "glu_pre_matrix", "glu_pre_transform",
     "glu_pre_source_map", "glu_pre_destroy", "glu_pre_read_mtx", "glu_pre_free",
@@ -76,7 +76,7 @@ class Stats(C.Structure):
                 ("sn_levels", C.c_uint32), ("sn_update_flops", C.c_double), ("sn_update_bytes", C.c_double),
                 ("sn_panel_bytes", C.c_double), ("sn_sweep_levels", C.c_uint32),
                 ("dense_update_bytes", C.c_double), ("dense_update_flops", C.c_double),
-                ("solve_launches", C.c_uint64)]
+                ("solve_launches", C.c_uint64), ("couple_columns", C.c_uint32), ("couple_groups", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -85,7 +85,7 @@ class Tuning(C.Structure):
                 ("solve_cluster", C.c_uint32), ("sn_width", C.c_uint32),
                 ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32), ("dense_tc_min", C.c_uint32),
                 ("dense_rate", C.c_uint32), ("sn_sweep_fused", C.c_uint32),
-                ("batch_tile", C.c_uint32)]
+                ("batch_tile", C.c_uint32), ("defer_tail", C.c_uint32)]
 
 
 _vp = C.c_void_p

@@ -14,7 +14,9 @@ factorization path in use reads --
   small supernodes into warps, the split between sparse part and dense
   trailing block (the cost model's dense rate and the largest buffered
   block), the width from which the dense block takes its panels in
-  look-ahead pairs, the width from which it updates on the tensor cores;
+  look-ahead pairs, the width from which it updates on the tensor cores,
+  how many of the sparse part's updates of the dense block are deferred to
+  tensor-core products after the sparse part;
 * column path (sn_width = 0): lanes per update, the cluster size of the
   narrow-level kernel, the work that sends a level to its own launch;
 * batched handles, in addition: the batch tile, the number of value sets one
@@ -43,6 +45,7 @@ SUPERNODAL_SPACE = {
     "dense_tail_max": [2048, 4096, 8192],
     "dense_lookahead": [0, 1024, 3072],
     "dense_tc_min": [0, 512, 1024, 2048],
+    "defer_tail": [0, 1, 4],
 }
 COLUMN_SPACE = {
     "group_lanes": [0, 8, 32],

