@@ -32,9 +32,12 @@
 //        warp 1   MMA issuer: 6 tcgen05.mma (M = N = 128, K = 8) per 8 of
 //                 K into one of two accumulator pairs (big, small), the
 //                 pair of the tile before being read meanwhile;
-//        warps 2-5 epilogue: load the C tile from HBM into registers while
-//                 the MMAs run, tcgen05.ld the tile's two sums, subtract
-//                 them, hand the pair back, store the tile.
+//        warps 2-9 epilogue (two per TMEM lane quarter, 64 columns each):
+//                 load the C tile into registers while the MMAs run,
+//                 tcgen05.ld the tile's two sums, subtract them, hand the
+//                 pair back, store the tile;
+//        warp 10  prefetch: each tile's C columns into L2 as soon as the
+//                 tile is drawn, so that the epilogue's loads hit L2.
 //      C stays where it lies (element (i, j) at val[doff[j] + i]), so in-place
 //      tails with irregular column offsets need no copy.
 // All waits on mbarriers are bounded (spin_limit polls); a wait that runs out
@@ -61,11 +64,14 @@ constexpr int kParts = 3;                                // TF32 parts of an ope
 constexpr int kPackRow = kParts * 128;                   // floats per pack row
 constexpr uint32_t kOpBytes = kTile * kChunk * 4;        // one operand part of one stage (16 KB)
 constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A0, A1, A2, B0, B1, B2
-constexpr int kThreads = 192;                            // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kEpiWarps = 8;                             // two per TMEM lane quarter, 64 columns each
+constexpr int kPrefetchWarp = 2 + kEpiWarps;             // C tiles into L2 ahead of the epilogue
+constexpr int kThreads = 32 * (3 + kEpiWarps);           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue, warp 10 prefetch
 constexpr uint32_t kTmemCols = 4 * kTile;                // two pairs (big, small) of FP32 accumulators
 constexpr size_t kBarBytes = 256;
 constexpr int kRing = 4;  // tile ids in flight between the producer and the other roles
-constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + 1024;  // + alignment slack
+constexpr size_t kOffBytes = sizeof(uint32_t) * kEpiWarps * 64;  // the epilogue warps' column offsets
+constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + kOffBytes + 1024;  // + alignment slack
 
 // Instruction descriptor of tcgen05.mma kind::tf32: D FP32 (bits 4-5 = 1), A
 // and B TF32 (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at
@@ -147,20 +153,31 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
                  : "memory");
 }
 
-// 32 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+// 32 consecutive FP32 columns at each of two TMEM addresses of this thread's
+// lane, one wait for both.
+__device__ __forceinline__ void tc_ld32x2(uint32_t ta, uint32_t tb, float (&va)[32], float (&vb)[32]) {
+    uint32_t r[64];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%64];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, "
+        "%45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%65];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(ta), "r"(tb)
+        : "memory");
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; ++i) {
+        va[i] = __uint_as_float(r[i]);
+        vb[i] = __uint_as_float(r[32 + i]);
+    }
 }
 
 // x rounded to TF32 (1 + 10 explicit significand bits), ties away from zero,
@@ -321,12 +338,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint64_t *full = bars;                   // [kStages] stage loaded (TMA bytes)
     uint64_t *empty = bars + kStages;        // [kStages] stage consumed (MMA commit)
     uint64_t *acc_full = bars + 2 * kStages;  // [2] accumulator ready (MMA commit)
-    uint64_t *acc_empty = acc_full + 2;       // [2] accumulator read (4 epilogue warps)
+    uint64_t *acc_empty = acc_full + 2;       // [2] accumulator read (the epilogue warps)
     uint64_t *done = acc_empty + 2;           // all MMAs of this CTA complete
     uint64_t *tile_full = done + 1;           // [kRing] tile id written (producer)
-    uint64_t *tile_empty = tile_full + kRing;  // [kRing] tile id read (MMA issuer + 4 epilogue warps)
+    uint64_t *tile_empty = tile_full + kRing;  // [kRing] tile id read (MMA issuer, epilogue and prefetch warps)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tile_empty + kRing);
     uint32_t *tile_id = tmem_slot + 1;        // [kRing]
+    uint32_t *epi_off = reinterpret_cast<uint32_t *>(smem + kStages * kStageBytes + kBarBytes);  // [warps][64]
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t total = tiles_r * tiles_c * count;
 
@@ -337,12 +355,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&acc_full[a], 1);
-            mbar_init(&acc_empty[a], 4);
+            mbar_init(&acc_empty[a], kEpiWarps);
         }
         mbar_init(done, 1);
         for (int j = 0; j < kRing; ++j) {
             mbar_init(&tile_full[j], 1);
-            mbar_init(&tile_empty[j], 5);
+            mbar_init(&tile_empty[j], 2 + kEpiWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
@@ -460,10 +478,46 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc_commit(done);
             if (!mbar_wait(done, 0, spin_limit)) atomicOr(status, DEV_TIMEOUT);
         }
+    } else if (warp == kPrefetchWarp) {
+        // ------------------------------------------------ C prefetch
+        // Each tile's C columns (128 rows, 512 bytes each) into L2 as soon as
+        // the producer has drawn the tile, up to kRing tiles ahead of the
+        // epilogue, whose loads then hit L2 instead of waiting on DRAM.
+        for (uint32_t i = 0;; ++i) {
+            const uint32_t slot = i % kRing, sph = (i / kRing) & 1;
+            if (!__all_sync(0xffffffffu, mbar_wait(&tile_full[slot], sph, spin_limit))) {
+                if (lane == 0) atomicOr(status, DEV_TIMEOUT);
+                break;
+            }
+            const uint32_t t = tile_id[slot];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tile_empty[slot]);
+            if (t >= total) break;
+            const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
+            const float *val = val_base + tl.z * stride;
+            const uint32_t rows = min(uint32_t(kTile), reg.r_hi - tl.rbase);
+            for (uint32_t cc = lane; cc < uint32_t(kTile); cc += 32) {
+                const uint32_t col = tl.cbase + cc;
+                if (col >= reg.c_hi) break;
+                const float *p0 = val + __ldg(doff + r0 + col) + r0 + tl.rbase;
+                const uintptr_t a0 = reinterpret_cast<uintptr_t>(p0) & ~uintptr_t(127);
+                const uintptr_t a1 = reinterpret_cast<uintptr_t>(p0 + rows - 1);
+                for (uintptr_t a = a0; a <= a1; a += 128)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+            }
+        }
     } else {
         // ------------------------------------------------ epilogue
-        const uint32_t q = warp & 3;           // TMEM lane quarter this warp may access
-        const uint32_t row = q * 32 + lane;    // tile row of this thread
+        // Warp w takes TMEM lane quarter w % 4 (the quarter a warp may
+        // access) and tile columns [64 h, 64 h + 64), h = (w - 2) / 4: two
+        // warps per quarter, so two per SM sub-partition hide each other's
+        // latencies.  Column offsets go through shared memory once per tile;
+        // interior tiles take a path without per-entry bounds.
+        const uint32_t ew = warp - 2;
+        const uint32_t q = warp & 3;
+        const uint32_t half = ew >> 2;
+        const uint32_t row = q * 32 + lane;  // tile row of this thread
+        uint32_t *soff = epi_off + ew * 64;
         if (reg.writeback) {
             // the factored diagonal block of the panel at wb_k0, kept in
             // scratch while that panel's blocks still read the original
@@ -471,7 +525,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (uint32_t z = blockIdx.x; z < count; z += gridDim.x) {
                 float *val = val_base + z * stride;
                 const float *ds = diag_scratch + size_t(z) * kDenseNB * kDenseNB;
-                for (uint32_t e = et; e < wb * wb; e += 128) {
+                for (uint32_t e = et; e < wb * wb; e += 32 * kEpiWarps) {
                     const uint32_t c = e / wb, rr = e - c * wb;
                     st_cg(val + doff[wk + c] + wk + rr, ds[c * kDenseNB + rr]);
                 }
@@ -490,25 +544,30 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (t >= total) break;
             const Tile tl = decode_tile(t, tiles_r, tiles_c, reg);
             float *val = val_base + tl.z * stride;
+            const uint32_t c0 = tl.cbase + half * 64;  // first tile column of this warp
+            const uint32_t ncol = c0 < reg.c_hi ? min(64u, reg.c_hi - c0) : 0u;
             const bool rok = tl.rbase + row < reg.r_hi;
+            const bool full_tile = __all_sync(0xffffffffu, rok) && ncol == 64;
             const uint32_t grow = r0 + tl.rbase + row;
-            // column offsets of the tile (lane j holds column j of each chunk)
-            uint32_t coff[4];
+            // column offsets of this warp's 64 columns (the previous tile's
+            // reads of them are done: the warp reached this point together)
+            for (uint32_t e = lane; e < 64; e += 32) soff[e] = e < ncol ? __ldg(doff + r0 + c0 + e) : 0u;
+            __syncwarp();
+            // C into registers while the MMAs run
+            float c[64];
+            if (full_tile) {
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                const uint32_t col = tl.cbase + cc * 32 + lane;
-                coff[cc] = col < reg.c_hi ? doff[r0 + col] : 0u;
-            }
-            // C tile row into registers while the MMAs run
-            float c[4][32];
-#pragma unroll
-            for (int cc = 0; cc < 4; ++cc)
-#pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const uint32_t o = __shfl_sync(0xffffffffu, coff[cc], jj);
-                    const bool ok = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
-                    c[cc][jj] = ok ? ld_cg(val + o + grow) : 0.0f;
+                for (int jj = 0; jj < 64; jj += 4) {
+                    const uint4 o = *reinterpret_cast<const uint4 *>(soff + jj);
+                    c[jj] = ld_cg(val + o.x + grow);
+                    c[jj + 1] = ld_cg(val + o.y + grow);
+                    c[jj + 2] = ld_cg(val + o.z + grow);
+                    c[jj + 3] = ld_cg(val + o.w + grow);
                 }
+            } else {
+#pragma unroll
+                for (int jj = 0; jj < 64; ++jj) c[jj] = (rok && uint32_t(jj) < ncol) ? ld_cg(val + soff[jj] + grow) : 0.0f;
+            }
             // the tile's two sums, subtracted in FP32: c := (c - big) - small
             const uint32_t a = u & 1, aph = (u >> 1) & 1;
             ++u;
@@ -518,29 +577,33 @@ __global__ void __launch_bounds__(kThreads, 1)
                 break;
             }
             tc_fence_after();
-            const uint32_t lane_base = tmem + ((q * 32) << 16) + a * 2 * kTile;
+            const uint32_t lane_base = tmem + ((q * 32) << 16) + a * 2 * kTile + half * 64;
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc) {
-                float acc[32];
-                tc_ld32(lane_base + cc * 32, acc);  // big
+            for (int cc = 0; cc < 2; ++cc) {
+                float big[32], sml[32];
+                tc_ld32x2(lane_base + cc * 32, lane_base + kTile + cc * 32, big, sml);
 #pragma unroll
-                for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
-                tc_ld32(lane_base + kTile + cc * 32, acc);  // small
-#pragma unroll
-                for (int jj = 0; jj < 32; ++jj) c[cc][jj] -= acc[jj];
+                for (int jj = 0; jj < 32; ++jj) c[cc * 32 + jj] = (c[cc * 32 + jj] - big[jj]) - sml[jj];
             }
             // the pair takes the tile after next while this one is stored
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acc_empty[a]);
+            if (full_tile) {
 #pragma unroll
-            for (int cc = 0; cc < 4; ++cc)
-#pragma unroll
-                for (int jj = 0; jj < 32; ++jj) {
-                    const uint32_t o = __shfl_sync(0xffffffffu, coff[cc], jj);
-                    const bool okc = rok && tl.cbase + cc * 32 + jj < reg.c_hi;
-                    if (okc) st_cg(val + o + grow, c[cc][jj]);
+                for (int jj = 0; jj < 64; jj += 4) {
+                    const uint4 o = *reinterpret_cast<const uint4 *>(soff + jj);
+                    st_cg(val + o.x + grow, c[jj]);
+                    st_cg(val + o.y + grow, c[jj + 1]);
+                    st_cg(val + o.z + grow, c[jj + 2]);
+                    st_cg(val + o.w + grow, c[jj + 3]);
                 }
+            } else if (rok) {
+#pragma unroll
+                for (int jj = 0; jj < 64; ++jj)
+                    if (uint32_t(jj) < ncol) st_cg(val + soff[jj] + grow, c[jj]);
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
