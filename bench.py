@@ -402,7 +402,7 @@ def plain_form(W, vals, local, nrhs, tensor_cores=False):
             ts.append(e0.elapsed_time(e1))
     ms = float(np.median(ts))
     form = ("one value set: FP32 refactor + FP32 solve of its right-hand sides, no refinement, "
-            + ("dense tail on the tensor cores (3xTF32)" if tensor_cores else "all updates FP32 FMA"))
+            + ("dense tail on the tensor cores (three-part BF16 split, FP32 accuracy)" if tensor_cores else "all updates FP32 FMA"))
     return {"value": nrhs / (ms / 1e3), "unit": "solves/s", "ms_per_matrix": ms, "form": form}
 
 

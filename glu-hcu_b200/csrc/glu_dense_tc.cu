@@ -2,35 +2,41 @@
 //
 // The blocked dense LU of the trailing block (glu_factor_dense.cu) spends
 // almost all of its flops in A22 -= L21 U12 with K = 64 or 128 (one panel or a
-// pair).  Here that product runs as tcgen05.mma kind::tf32 with FP32 accuracy
-// kept by splitting every operand into three TF32 parts,
-//     a = a0 + a1 + a2,  a0 = rna_tf32(a), a1 = rna_tf32(a - a0),
-//                        a2 = rna_tf32(a - a0 - a1)
-// (exact: 3 x 11 significant bits cover FP32's 24), and keeping every
-// product term down to 2^-22 relative:
-//     a b ~= a0 b0 + (a0 b1 + a1 b0) + (a0 b2 + a1 b1 + a2 b0),
-// whose error, below 2^-32 |a b|, is far under FP32 rounding.  The big term
-// a0 b0 (exact in FP32) and the small terms go to separate FP32 accumulators
-// in tensor memory over the whole K of the update (16 MMAs of K = 8 for a
-// panel pair), so the small terms' truncating accumulation stays 2^-11 below
-// the big one's; the tile's two sums are then subtracted from the entry in
-// FP32 with round to nearest, c := (c - big) - small.  The big sum takes one
-// truncation per MMA (K / 8 in all; the FMA kernel rounds once per product),
-// and the tile's C is read and written once.
+// pair), and the deferred coupling of the sparse part adds products of the
+// same form.  Here that product runs as tcgen05.mma kind::f16 on BF16
+// operands with FP32 accuracy kept by splitting every operand into three BF16
+// parts,
+//     a = a0 + a1 + a2,  a0 = rna_bf16(a), a1 = rna_bf16(a - a0),
+//                        a2 = a - a0 - a1
+// (exact: a - a0 has at most 15 significant bits, a - a0 - a1 at most 7, so
+// 3 x 8 bits cover FP32's 24), and keeping every product term down to
+// 2^-24 relative:
+//     a b ~= a0 b0 + (a0 b1 + a1 b0) + (a0 b2 + a1 b1 + a2 b0) + (a1 b2 + a2 b1),
+// whose error, about 2^-32 |a b|, is far under FP32 rounding -- 8 BF16 MMAs
+// per 16 of K, two thirds of the tensor time of the 6 TF32 products a TF32
+// split needs for the same accuracy, and half its operand bytes.  The big
+// term a0 b0 (exact in FP32) and the small terms go to separate FP32
+// accumulators in tensor memory over the whole K of the update (8 MMAs of K =
+// 16 for a panel pair), so the small terms' truncating accumulation stays
+// 2^-8 below the big one's; the tile's two sums are then subtracted from the
+// entry in FP32 with round to nearest, c := (c - big) - small.  The big sum
+// takes one truncation per MMA (K / 16 in all; the FMA kernel rounds once per
+// product), and the tile's C is read and written once.
 
 // Data flow per update:
 //   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
-//      split into their three TF32 parts, written K-major as rows of 384
-//      floats (slots 0..127 part 0, 128..255 part 1, 256..383 part 2; the
-//      first panel of a pair fills slots 0..63 of each part, the second
+//      split into their three BF16 parts, written K-major as rows of 384
+//      BF16 values (slots 0..127 part 0, 128..255 part 1, 256..383 part 2;
+//      the first panel of a pair fills slots 0..63 of each part, the second
 //      64..127) -- the operand layout the MMA reads.
 //   2. k_dense_update_tc, persistent (one CTA per SM), per 128 x 128 tile of
 //      the trailing block:
-//        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 32 FP32
+//        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 64 BF16
 //                 operand boxes (128-byte swizzle), three parts of A and of B
-//                 per 32-wide K chunk, into a 2-stage ring;
-//        warp 1   MMA issuer: 6 tcgen05.mma (M = N = 128, K = 8) per 8 of
-//                 K into one of two accumulator pairs (big, small), the
+//                 per 64-wide K chunk, into a 2-stage ring (a panel pair's
+//                 whole K);
+//        warp 1   MMA issuer: 8 tcgen05.mma (M = N = 128, K = 16) per 16
+//                 of K into one of two accumulator pairs (big, small), the
 //                 pair of the tile before being read meanwhile;
 //        warps 2-9 epilogue (two per TMEM lane quarter, 64 columns each):
 //                 load the C tile into registers while the MMAs run,
@@ -58,11 +64,11 @@ namespace glu {
 namespace {
 
 constexpr int kTile = 128;                               // M = N of an update tile
-constexpr int kChunk = 32;                               // K per stage: one 128-byte row of FP32
+constexpr int kChunk = 64;                               // K per stage: one 128-byte row of BF16
 constexpr int kStages = 2;
-constexpr int kParts = 3;                                // TF32 parts of an operand
-constexpr int kPackRow = kParts * 128;                   // floats per pack row
-constexpr uint32_t kOpBytes = kTile * kChunk * 4;        // one operand part of one stage (16 KB)
+constexpr int kParts = 3;                                // BF16 parts of an operand
+constexpr int kPackRow = kParts * 128;                   // BF16 values per pack row
+constexpr uint32_t kOpBytes = kTile * kChunk * 2;        // one operand part of one stage (16 KB)
 constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A0, A1, A2, B0, B1, B2
 constexpr int kEpiWarps = 8;                             // two per TMEM lane quarter, 64 columns each
 constexpr int kPrefetchWarp = 2 + kEpiWarps;             // C tiles into L2 ahead of the epilogue
@@ -73,10 +79,10 @@ constexpr int kRing = 4;  // tile ids in flight between the producer and the oth
 constexpr size_t kOffBytes = sizeof(uint32_t) * kEpiWarps * 64;  // the epilogue warps' column offsets
 constexpr size_t kSmemBytes = kStages * kStageBytes + kBarBytes + kOffBytes + 1024;  // + alignment slack
 
-// Instruction descriptor of tcgen05.mma kind::tf32: D FP32 (bits 4-5 = 1), A
-// and B TF32 (bits 7-9, 10-12 = 2), both K-major (bits 15, 16 = 0), N >> 3 at
+// Instruction descriptor of tcgen05.mma kind::f16: D FP32 (bits 4-5 = 1), A
+// and B BF16 (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
 // bits 17-22, M >> 4 at bits 24-28.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(kTile >> 3) << 17) |
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kTile >> 3) << 17) |
                             (uint32_t(kTile >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -84,7 +90,7 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p) {
 }
 
 // Shared-memory matrix descriptor of a K-major operand tile in the canonical
-// 128-byte-swizzled layout written by a TMA box of 32 FP32 x rows: rows of
+// 128-byte-swizzled layout written by a TMA box of 64 BF16 x rows: rows of
 // 128 bytes, 8-row groups 1024 bytes apart (stride byte offset), layout type 2
 // (128-byte swizzle) at bits 61-63, descriptor version 1 at bits 46-47.  The
 // leading byte offset is unused for swizzled K-major layouts.
@@ -138,11 +144,11 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
+__device__ __forceinline__ void tc_mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(accumulate)
         : "memory");
 }
@@ -180,14 +186,27 @@ __device__ __forceinline__ void tc_ld32x2(uint32_t ta, uint32_t tb, float (&va)[
     }
 }
 
-// x rounded to TF32 (1 + 10 explicit significand bits), ties away from zero,
-// as an FP32 value whose 13 low significand bits are zero: adding half a TF32
-// unit in the last place to the magnitude bits and clearing the 13 bits
-// below it (a carry into the exponent is the correct rounding up).  Done on
-// the bits so that every part of the split is exactly representable in TF32
-// whatever a conversion instruction leaves in the low bits; finite inputs.
-__device__ __forceinline__ float tf32_rna(float x) {
-    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+// x rounded to BF16 (1 + 7 explicit significand bits), ties away from zero,
+// as the bits of an FP32 value whose 16 low bits are zero: half a BF16 unit
+// in the last place added to the magnitude bits, the 16 bits below it cleared
+// (a carry into the exponent is the correct rounding up).  Done on the bits so
+// that every part of the split is exact; finite inputs.
+__device__ __forceinline__ uint32_t bf16_rna_bits(float x) { return (__float_as_uint(x) + 0x8000u) & 0xFFFF0000u; }
+
+// The three BF16 parts of four FP32 values, each part's four as one 8-byte
+// word (value u in bits 16 u .. 16 u + 15).
+__device__ __forceinline__ void split_bf16x4(const float (&v)[4], uint2 &p0, uint2 &p1, uint2 &p2) {
+    uint32_t b[3][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        b[0][u] = bf16_rna_bits(v[u]);
+        const float r1 = v[u] - __uint_as_float(b[0][u]);  // exact
+        b[1][u] = bf16_rna_bits(r1);
+        b[2][u] = __float_as_uint(r1 - __uint_as_float(b[1][u]));  // exact, at most 7 significant bits
+    }
+    p0 = make_uint2((b[0][0] >> 16) | (b[0][1] & 0xFFFF0000u), (b[0][2] >> 16) | (b[0][3] & 0xFFFF0000u));
+    p1 = make_uint2((b[1][0] >> 16) | (b[1][1] & 0xFFFF0000u), (b[1][2] >> 16) | (b[1][3] & 0xFFFF0000u));
+    p2 = make_uint2((b[2][0] >> 16) | (b[2][1] & 0xFFFF0000u), (b[2][2] >> 16) | (b[2][3] & 0xFFFF0000u));
 }
 
 struct Tile {
@@ -209,19 +228,19 @@ __device__ __forceinline__ Tile decode_tile(uint32_t t, uint32_t tiles_r, uint32
 // ---------------------------------------------------------------- pack --
 // Rows [r_start, m) of the panel's L21 (columns k0 .. k0 + kb - 1) and
 // columns [r_start, m) of its U12 (rows k0 .. k0 + kb - 1), split into three
-// TF32 parts: pack[z][i][128 * p + slot0 + k] = part p, for k < 64 (zero for
+// BF16 parts: pack[z][i][128 * p + slot0 + k] = part p, for k < 64 (zero for
 // k >= kb).  Blocks [0, nA) take 128 rows of L21 each, the rest 128 columns of
 // U12; blockIdx.z selects the value set.
 __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ val_base, uint64_t stride,
                                                     const uint32_t *__restrict__ doff, uint32_t m, uint32_t k0,
                                                     uint32_t kb, uint32_t slot0, uint32_t r_start, uint32_t nA,
-                                                    float *__restrict__ packA, float *__restrict__ packB) {
+                                                    uint16_t *__restrict__ packA, uint16_t *__restrict__ packB) {
     __shared__ float sT[kDenseNB][kTile + 1];
     const float *val = val_base + blockIdx.z * stride;
     const uint32_t tid = threadIdx.x;
     const uint32_t r = tid >> 1, h = tid & 1;  // writer: row (or column) r, K half h
     float x[32];
-    float *dst = nullptr;
+    uint16_t *dst = nullptr;
     if (blockIdx.x < nA) {
         const uint32_t row0 = r_start + blockIdx.x * kTile;
         for (uint32_t e = tid; e < uint32_t(kDenseNB) * kTile; e += blockDim.x) {
@@ -243,19 +262,12 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
     }
 #pragma unroll
     for (int i = 0; i < 32; i += 4) {
-        float4 p0, p1, p2;
-        float *a0 = &p0.x, *a1 = &p1.x, *a2 = &p2.x;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const float v = x[i + u];
-            a0[u] = tf32_rna(v);
-            const float r1 = v - a0[u];  // exact
-            a1[u] = tf32_rna(r1);
-            a2[u] = tf32_rna(r1 - a1[u]);  // r1 - a1 exact, and at most 11 bits remain
-        }
-        *reinterpret_cast<float4 *>(dst + i) = p0;
-        *reinterpret_cast<float4 *>(dst + 128 + i) = p1;
-        *reinterpret_cast<float4 *>(dst + 256 + i) = p2;
+        const float v[4] = {x[i], x[i + 1], x[i + 2], x[i + 3]};
+        uint2 p0, p1, p2;
+        split_bf16x4(v, p0, p1, p2);
+        *reinterpret_cast<uint2 *>(dst + i) = p0;
+        *reinterpret_cast<uint2 *>(dst + 128 + i) = p1;
+        *reinterpret_cast<uint2 *>(dst + 256 + i) = p2;
     }
 }
 
@@ -270,7 +282,7 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
 // k_s's CSR entries [ustart[g][b], ustart[g][b + 1]), the ones in those
 // columns (their CSC positions from cpos).  The start tables (nblk + 1 entries
 // per slot) are computed with the plan.  A 128 x 128 tile in shared memory,
-// then coalesced writes of the three parts.
+// then coalesced writes of the three BF16 parts.
 constexpr uint32_t kCoupleLd = kTile + 1;
 constexpr size_t kCoupleSmem = sizeof(float) * kTile * kCoupleLd;
 
@@ -281,7 +293,7 @@ __global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restric
                                                        uint32_t t, uint32_t m, uint32_t ncols, uint32_t slot0,
                                                        const uint32_t *__restrict__ lstart,
                                                        const uint32_t *__restrict__ ustart, uint32_t nblk,
-                                                       float *__restrict__ packA, float *__restrict__ packB) {
+                                                       uint16_t *__restrict__ packA, uint16_t *__restrict__ packB) {
     extern __shared__ float sT[];  // [128][kCoupleLd]: sT[r * kCoupleLd + s]
     const float *val = val_base + blockIdx.z * stride;
     const uint32_t tid = threadIdx.x;
@@ -300,24 +312,18 @@ __global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restric
         }
     }
     __syncthreads();
-    float *pack = aside ? packA : packB;
+    uint16_t *pack = aside ? packA : packB;
     const uint32_t rows = min(uint32_t(kTile), m - b0);
     for (uint32_t e = tid; e < rows * (kTile / 4); e += kTile) {
         const uint32_t r = e / (kTile / 4), q = e - r * (kTile / 4);
-        float4 p0, p1, p2;
-        float *a0 = &p0.x, *a1 = &p1.x, *a2 = &p2.x;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const float v = sT[r * kCoupleLd + 4 * q + u];
-            a0[u] = tf32_rna(v);
-            const float r1 = v - a0[u];
-            a1[u] = tf32_rna(r1);
-            a2[u] = tf32_rna(r1 - a1[u]);
-        }
-        float *dst = pack + (size_t(blockIdx.z) * m + b0 + r) * kPackRow + 4 * q;
-        *reinterpret_cast<float4 *>(dst) = p0;
-        *reinterpret_cast<float4 *>(dst + 128) = p1;
-        *reinterpret_cast<float4 *>(dst + 256) = p2;
+        const float *src = sT + r * kCoupleLd + 4 * q;
+        const float v[4] = {src[0], src[1], src[2], src[3]};
+        uint2 p0, p1, p2;
+        split_bf16x4(v, p0, p1, p2);
+        uint16_t *dst = pack + (size_t(blockIdx.z) * m + b0 + r) * kPackRow + 4 * q;
+        *reinterpret_cast<uint2 *>(dst) = p0;
+        *reinterpret_cast<uint2 *>(dst + 128) = p1;
+        *reinterpret_cast<uint2 *>(dst + 256) = p2;
     }
 }
 
@@ -453,21 +459,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                     tc_fence_after();
                     const uint32_t base = smem_addr(smem + s * kStageBytes);
 #pragma unroll
-                    for (uint32_t k8 = 0; k8 < kChunk / 8; ++k8) {
-                        const uint32_t off = k8 * 32;  // 8 TF32 values = 32 bytes along K
+                    for (uint32_t k16 = 0; k16 < kChunk / 16; ++k16) {
+                        const uint32_t off = k16 * 32;  // 16 BF16 values = 32 bytes along K
                         uint64_t A[kParts], B[kParts];
 #pragma unroll
                         for (int p = 0; p < kParts; ++p) {
                             A[p] = kmajor_sw128_desc(base + p * kOpBytes + off);
                             B[p] = kmajor_sw128_desc(base + (kParts + p) * kOpBytes + off);
                         }
-                        const uint32_t acc = (kc | k8) != 0;
-                        tc_mma_tf32(d_small, A[2], B[0], acc);  // 2^-22 terms first
-                        tc_mma_tf32(d_small, A[1], B[1], 1);
-                        tc_mma_tf32(d_small, A[0], B[2], 1);
-                        tc_mma_tf32(d_small, A[1], B[0], 1);  // 2^-11 terms
-                        tc_mma_tf32(d_small, A[0], B[1], 1);
-                        tc_mma_tf32(d_big, A[0], B[0], acc);
+                        const uint32_t acc = (kc | k16) != 0;
+                        tc_mma_bf16(d_small, A[1], B[2], acc);  // 2^-24 terms first
+                        tc_mma_bf16(d_small, A[2], B[1], 1);
+                        tc_mma_bf16(d_small, A[0], B[2], 1);  // 2^-16 terms
+                        tc_mma_bf16(d_small, A[1], B[1], 1);
+                        tc_mma_bf16(d_small, A[2], B[0], 1);
+                        tc_mma_bf16(d_small, A[0], B[1], 1);  // 2^-8 terms
+                        tc_mma_bf16(d_small, A[1], B[0], 1);
+                        tc_mma_bf16(d_big, A[0], B[0], acc);
                     }
                     tc_commit(&empty[s]);
                 }
@@ -630,21 +638,21 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 }  // namespace
 
-cudaError_t dense_tc_tensor_map(float *pack, uint32_t m, uint32_t batch, CUtensorMap *map) {
+cudaError_t dense_tc_tensor_map(uint16_t *pack, uint32_t m, uint32_t batch, CUtensorMap *map) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (!enc) return cudaErrorNotSupported;
     const cuuint64_t dims[3] = {cuuint64_t(kPackRow), m, batch};
-    const cuuint64_t strides[2] = {kPackRow * sizeof(float), cuuint64_t(m) * kPackRow * sizeof(float)};
+    const cuuint64_t strides[2] = {kPackRow * sizeof(uint16_t), cuuint64_t(m) * kPackRow * sizeof(uint16_t)};
     const cuuint32_t box[3] = {uint32_t(kChunk), uint32_t(kTile), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pack, dims, strides, box, estr,
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, pack, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count, const uint32_t *doff, uint32_t m,
-                              uint32_t k0, uint32_t kb, uint32_t slot0, float *packA, float *packB,
+                              uint32_t k0, uint32_t kb, uint32_t slot0, uint16_t *packA, uint16_t *packB,
                               cudaStream_t st) {
     const uint32_t r_start = k0 + kb;
     if (r_start >= m) return cudaSuccess;
@@ -693,7 +701,7 @@ cudaError_t launch_dense_update_tc(const CUtensorMap &mapA, const CUtensorMap &m
 
 cudaError_t launch_couple_pack(const DevPattern &P, const float *val, uint64_t stride, uint32_t count, uint32_t t,
                                uint32_t m, uint32_t ncols, uint32_t slot0, const uint32_t *lstart,
-                               const uint32_t *ustart, float *packA, float *packB, cudaStream_t st) {
+                               const uint32_t *ustart, uint16_t *packA, uint16_t *packB, cudaStream_t st) {
     if (m == 0 || ncols == 0) return cudaSuccess;
     if (ncols > uint32_t(kTile)) return cudaErrorInvalidValue;
     static PerDeviceOnce attr;

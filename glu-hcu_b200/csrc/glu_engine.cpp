@@ -241,7 +241,7 @@ struct glu_handle_s {
     // panel-done / rest-done events
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_panel = nullptr, ev_rest = nullptr;
-    // tensor-core dense update: TF32 hi/lo operand packs and their TMA maps
+    // tensor-core dense update: BF16 three-part operand packs and their TMA maps
     // (allocated on the first factorization that uses them)
     DevBuf d_packA, d_packB, d_tc_counter;
     // inverses of the dense tail's 64 x 64 diagonal blocks (L and U) per value
@@ -333,7 +333,7 @@ constexpr uint32_t kDenseTcMin = 1024;
 // Cost of one deferred coupling product (up to 128 columns over the whole
 // m x m dense block), in scattered supernode-update entries per entry of the
 // block.
-constexpr double kCoupleGroupCost = 1.0;
+constexpr double kCoupleGroupCost = 0.25;
 constexpr double kSparseRate = 0.2e12, kLevelLatency = 8e-6;
 
 uint32_t choose_split(const SymbolicData &s, const std::vector<int32_t> &level_ptr,
@@ -1662,11 +1662,11 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
     // allocated once per handle
     const bool tc = h->m && h->tune.dense_tc_min && h->m >= h->tune.dense_tc_min;
     if (tc && h->pack_m != h->m) {
-        const size_t pack_bytes = sizeof(float) * kDensePackRow * size_t(h->m) * h->batch;
+        const size_t pack_bytes = sizeof(uint16_t) * kDensePackRow * size_t(h->m) * h->batch;
         GLU_CUDA(h->d_packA.alloc(pack_bytes), "allocate tensor-core operand packs");
         GLU_CUDA(h->d_packB.alloc(pack_bytes), "allocate tensor-core operand packs");
-        GLU_CUDA(dense_tc_tensor_map(h->d_packA.as<float>(), h->m, h->batch, &h->map_packA), "tensor map");
-        GLU_CUDA(dense_tc_tensor_map(h->d_packB.as<float>(), h->m, h->batch, &h->map_packB), "tensor map");
+        GLU_CUDA(dense_tc_tensor_map(h->d_packA.as<uint16_t>(), h->m, h->batch, &h->map_packA), "tensor map");
+        GLU_CUDA(dense_tc_tensor_map(h->d_packB.as<uint16_t>(), h->m, h->batch, &h->map_packB), "tensor map");
         GLU_CUDA(h->d_tc_counter.alloc(sizeof(uint32_t) * 2), "allocate tile counters");
         h->pack_m = h->m;
     }
@@ -1683,7 +1683,7 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
             GLU_LAUNCH(KK_COUPLE_PACK,
                        launch_couple_pack(h->P, val, stride, count, h->t, h->m, nc, gr.c0,
                                           h->d_couple_lstart.as<uint32_t>(), h->d_couple_ustart.as<uint32_t>(),
-                                          h->d_packA.as<float>(), h->d_packB.as<float>(), st),
+                                          h->d_packA.as<uint16_t>(), h->d_packB.as<uint16_t>(), st),
                        "factor (coupling pack)");
             GLU_LAUNCH(KK_UPDATE_TC,
                        launch_couple_update_tc(h->map_packA, h->map_packB, dbase, dstride, count, doff, h->m, nc,
@@ -1726,23 +1726,24 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         ++nlaunch;
         return e;
     };
-    // TF32 hi/lo operands of panel k0 (slot0 0: first of a pair or alone; 64:
+    // BF16 three-part operands of panel k0 (slot0 0: first of a pair or alone; 64:
     // second of a pair), on the panel stream
     auto pack = [&](uint32_t k0, uint32_t kb, uint32_t slot0, bool needed) -> cudaError_t {
         if (!needed) return cudaSuccess;
         cudaError_t e = pf.begin(ps);
         if (e == cudaSuccess)
-            e = launch_dense_pack(dbase, dstride, count, doff, h->m, k0, kb, slot0, h->d_packA.as<float>(),
-                                  h->d_packB.as<float>(), ps);
+            e = launch_dense_pack(dbase, dstride, count, doff, h->m, k0, kb, slot0, h->d_packA.as<uint16_t>(),
+                                  h->d_packB.as<uint16_t>(), ps);
         if (e == cudaSuccess) e = pf.end(KK_PACK, ps);
         ++nlaunch;
         return e;
     };
     auto panel = [&](uint32_t k0, uint32_t kb) -> cudaError_t {
         cudaError_t e = pf.begin(ps);
-        if (e == cudaSuccess) e = launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, ps);
+        if (e == cudaSuccess)
+            e = launch_dense_panel(dbase, dstride, count, doff, h->m, k0, kb, pert, dscr, 0, h->num_sms, ps);
         if (e == cudaSuccess) e = pf.end(KK_PANEL, ps);
-        ++nlaunch;
+        nlaunch += dense_panel_launches(count, h->m, k0, kb, h->num_sms);
         return e;
     };
     for (uint32_t k0 = 0; k0 < h->m;) {

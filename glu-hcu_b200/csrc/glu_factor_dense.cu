@@ -29,7 +29,11 @@ namespace glu {
 // rows of L21 (x U11 = a), the rest 128 columns of U12 (L11 x = a), one per
 // thread, chunked (tri_rows_solve).  The rows or columns are copied to shared
 // memory asynchronously while the diagonal block is factored.  blockIdx.z
-// selects the value set.
+// selects the value set.  With from_scratch set, block b of the launch is
+// block b + 1 of the step and takes the diagonal block already factored into
+// diag_scratch by a launch of block 0 alone (the same code, so the same
+// values) instead of factoring it again: for many value sets the redundant
+// factorizations would outweigh the row solves.
 constexpr int kPW = kPanelRows + 1;  // leading dimension of the panel work tile
 constexpr size_t kPanelSmem =
     sizeof(float) * (size_t(kDenseNB) * kPW + size_t(kDenseNB) * kTriML + 2 * kTriMax) + sizeof(uint32_t) * kDenseNB;
@@ -39,7 +43,8 @@ static_assert(2 * kPanelRows == kTriThreads, "128 rows per panel block");
 __global__ void __launch_bounds__(kTriThreads) k_dense_panel(float *val_base, uint64_t stride,
                                                              const uint32_t *__restrict__ doff, uint32_t m,
                                                              uint32_t k0, uint32_t kb, const float *pert_z,
-                                                             float *diag_scratch, uint32_t last_has_l, uint32_t nL) {
+                                                             float *diag_scratch, uint32_t last_has_l, uint32_t nL,
+                                                             uint32_t from_scratch) {
     extern __shared__ float4 psm4[];
     float *sW = reinterpret_cast<float *>(psm4);  // [k][thread]: rows of L21 or columns of U12
     float *sM = sW + kDenseNB * kPW;               // U11 (row-major, pivot reciprocals in the padding) or L11^T
@@ -47,7 +52,7 @@ __global__ void __launch_bounds__(kTriThreads) k_dense_panel(float *val_base, ui
     uint32_t *sCol = reinterpret_cast<uint32_t *>(sM + kDenseNB * kTriML + 2 * kTriMax);
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
-    const uint32_t tid = threadIdx.x, b = blockIdx.x;
+    const uint32_t tid = threadIdx.x, b = blockIdx.x + from_scratch;
     const uint32_t r0 = k0 + kb;
     if (tid < kb) sCol[tid] = doff[k0 + tid] + k0;
     // this block's rows (columns) of the panel, in flight during the LU
@@ -70,13 +75,22 @@ __global__ void __launch_bounds__(kTriThreads) k_dense_panel(float *val_base, ui
     // the diagonal block
     const uint32_t row = tid >> 2, q = tid & 3;
     float a[kTriChunk];
+    if (from_scratch) {
+        const float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
 #pragma unroll
-    for (int jj = 0; jj < kTriChunk; ++jj) {
-        const uint32_t cc = q * kTriChunk + jj;
-        a[jj] = (row < kb && cc < kb) ? ld_cg(val + sCol[cc] + row) : 0.0f;
+        for (int jj = 0; jj < kTriChunk; ++jj) {
+            const uint32_t cc = q * kTriChunk + jj;
+            a[jj] = (row < kb && cc < kb) ? ld_cg(ds + cc * kDenseNB + row) : 0.0f;
+        }
+    } else {
+#pragma unroll
+        for (int jj = 0; jj < kTriChunk; ++jj) {
+            const uint32_t cc = q * kTriChunk + jj;
+            a[jj] = (row < kb && cc < kb) ? ld_cg(val + sCol[cc] + row) : 0.0f;
+        }
+        // a pivot is perturbed only when its column has an L part
+        tri_diag_lu(a, kb, (r0 < m) || last_has_l, pert, urow);
     }
-    // a pivot is perturbed only when its column has an L part
-    tri_diag_lu(a, kb, (r0 < m) || last_has_l, pert, urow);
     if (b == 0) {
         float *ds = diag_scratch + size_t(blockIdx.z) * kDenseNB * kDenseNB;
 #pragma unroll
@@ -248,9 +262,14 @@ __global__ void __launch_bounds__(256, 2) k_dense_update(float *val_base, uint64
     }
 }
 
+uint32_t dense_panel_launches(uint32_t count, uint32_t m, uint32_t k0, uint32_t kb, uint32_t num_sms) {
+    const uint32_t nL = (m - (k0 + kb) + kPanelRows - 1) / kPanelRows;
+    return (nL && uint64_t(count) * (1 + 2 * nL) > 4ull * num_sms) ? 2u : 1u;
+}
+
 cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, const uint32_t *doff,
                                uint32_t m, uint32_t k0, uint32_t kb, const float *pert_z,
-                               float *diag_scratch, uint32_t last_has_l, cudaStream_t st) {
+                               float *diag_scratch, uint32_t last_has_l, uint32_t num_sms, cudaStream_t st) {
     static PerDeviceOnce attr;
     cudaError_t e = attr.run([] {
         return cudaFuncSetAttribute(k_dense_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPanelSmem));
@@ -259,9 +278,20 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
     uint32_t rest = m - (k0 + kb);
     uint32_t nL = (rest + kPanelRows - 1) / kPanelRows;
     uint32_t nU = nL;
+    // more blocks than a few waves: factor the diagonal blocks once, then the
+    // rows and columns from them (one launch more, the LU not repeated per block)
+    if (dense_panel_launches(count, m, k0, kb, num_sms) == 2) {
+        k_dense_panel<<<dim3(1, 1, count), kTriThreads, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z,
+                                                                           diag_scratch, last_has_l, nL, 0);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        k_dense_panel<<<dim3(nL + nU, 1, count), kTriThreads, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z,
+                                                                                 diag_scratch, last_has_l, nL, 1);
+        return cudaGetLastError();
+    }
     dim3 grid(1 + nL + nU, 1, count);
     k_dense_panel<<<grid, kTriThreads, kPanelSmem, st>>>(val, stride, doff, m, k0, kb, pert_z, diag_scratch,
-                                                          last_has_l, nL);
+                                                          last_has_l, nL, 0);
     return cudaGetLastError();
 }
 

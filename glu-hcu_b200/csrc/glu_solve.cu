@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kRB) k_dense_diag_inv(const float *__restrict_
 }
 
 template <int kMode>
-__global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ val, const uint32_t *__restrict__ doff,
+__global__ void __launch_bounds__(256, 4) k_dense_trsv(const float *__restrict__ val, const uint32_t *__restrict__ doff,
                                                     uint32_t t, uint32_t m, float *y, uint32_t n, uint32_t nrhs,
                                                     uint32_t *flags, uint32_t *ticket, uint32_t *status,
                                                     uint32_t spin_limit, uint32_t ticket_base, uint64_t dstride,
@@ -285,13 +285,8 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
     auto T = [&](uint32_t i, uint32_t c) -> float {
         return kTrans ? val[doff[i] + c] : val[doff[c] + i];
     };
-    // the diagonal block's inverse does not depend on x either: its loads are
-    // issued first (row-major; transposed for the transposed sweeps)
     constexpr int kTilePer = kRB * kRB / 256;
-    float dv[kTilePer];
-    const float *inv = dinv + ((size_t(z) * nb + b) * 2 + kWhich) * kRB * kRB;
-#pragma unroll
-    for (int qq = 0; qq < kTilePer; ++qq) dv[qq] = __ldg(inv + tid + qq * 256);
+    const float *inv = dinv + ((size_t(z) * nb + b) * 2 + kWhich) * kRB * kRB;  // row-major
     // tile T(rb0.., block s in solve order): independent of x
     auto load_tile = [&](uint32_t s, float (&tv)[kTilePer]) {
         const uint32_t c = kLower ? s : nb - 1 - s;
@@ -315,11 +310,12 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
             const uint32_t c = kLower ? s : nb - 1 - s;
             const uint32_t cb0 = c * kRB, cb1 = min(cb0 + kRB, m);
             if (s + 1 < tk) load_tile(s + 1, tn);
+            if (kTrans) {  // transposed: through shared memory, loads coalesced along the rows
 #pragma unroll
-            for (int qq = 0; qq < kTilePer; ++qq) {
-                const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
-                const uint32_t i = kTrans ? a : bb, cc = kTrans ? bb : a;
-                tile[i][cc] = tv[qq];
+                for (int qq = 0; qq < kTilePer; ++qq) {
+                    const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;
+                    tile[a][bb] = tv[qq];
+                }
             }
             if (tid == 0) wait_count(flags + c, 1u, status, spin_limit);
             __syncthreads();
@@ -330,11 +326,20 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
                 xs[cc][r] = v;
             }
             __syncthreads();
+            if (kTrans) {
 #pragma unroll 4
-            for (uint32_t cc = q * 16; cc < q * 16 + 16; ++cc) {
-                float tv2 = tile[row][cc];
+                for (uint32_t cc = q * 16; cc < q * 16 + 16; ++cc) {
+                    float tv2 = tile[row][cc];
 #pragma unroll
-                for (int r = 0; r < kRHSChunk; ++r) acc[r] = fmaf(tv2, xs[cc][r], acc[r]);
+                    for (int r = 0; r < kRHSChunk; ++r) acc[r] = fmaf(tv2, xs[cc][r], acc[r]);
+                }
+            } else {  // thread (row, q) holds T(row, q + 4 j), j < 16: multiplied in registers
+#pragma unroll
+                for (int qq = 0; qq < kTilePer; ++qq) {
+                    const uint32_t cc = q + 4 * qq;
+#pragma unroll
+                    for (int r = 0; r < kRHSChunk; ++r) acc[r] = fmaf(tv[qq], xs[cc][r], acc[r]);
+                }
             }
             __syncthreads();
 #pragma unroll
@@ -346,10 +351,11 @@ __global__ void __launch_bounds__(256) k_dense_trsv(const float *__restrict__ va
 #pragma unroll
         for (int qq = 0; qq < kTilePer; ++qq) {
             const uint32_t e = tid + qq * 256, a = e / kRB, bb = e % kRB;  // inverse element (a, bb)
+            const float dv = __ldg(inv + e);
             if (kTrans)
-                tile[bb][a] = dv[qq];
+                tile[bb][a] = dv;
             else
-                tile[a][bb] = dv[qq];
+                tile[a][bb] = dv;
         }
         __syncthreads();
         if (tid < kRB * kRHSChunk) {

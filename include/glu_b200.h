@@ -293,7 +293,7 @@ typedef struct {
                                   (0: never)                                     */
     uint32_t dense_tc_min;     /* dense trailing blocks at least this wide update
                                   on the tensor cores (tcgen05, FP32 accuracy by
-                                  a three-part TF32 split), each update region
+                                  a three-part BF16 split), each update region
                                   whose area over the value sets reaches
                                   min(dense_tc_min^2, two 128 x 128 tiles per
                                   SM); 0: FP32 FMA always                      */

@@ -1,4 +1,4 @@
-"""The tensor-core trailing update of the dense tail (tcgen05, 3xTF32) against
+"""The tensor-core trailing update of the dense tail (tcgen05, three-part BF16 split) against
 the oracle's FP32 column algorithm.
 
 The tensor-core path is forced on small trailing blocks (dense_tc_min low) so
