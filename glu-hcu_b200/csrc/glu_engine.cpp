@@ -1046,7 +1046,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->nnz = s.nnz;
     h->batch = batch;
     h->pat = std::move(s);
-    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 1u,
+    h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 0u,
                          0u, 1u};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");

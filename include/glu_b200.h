@@ -300,9 +300,12 @@ typedef struct {
     uint32_t dense_rate;       /* dense-block throughput (GFLOP/s) the split cost
                                   model assumes; 0: built in (FMA or tensor-core
                                   rate, whichever the block would use)           */
-    uint32_t sn_sweep_fused;   /* 1: each supernodal solve sweep is one launch in
+    uint32_t sn_sweep_fused;   /* 0 (default): one launch per supernodal solve
+                                  sweep level; 1: each sweep is one launch in
                                   which a supernode waits (bounded) for the ones
-                                  that update it; 0: one launch per sweep level  */
+                                  that update it (slower on the patterns
+                                  measured: the ticket and the waits cost more
+                                  than the level launches)                      */
     uint32_t batch_tile;       /* value sets one supernode-update block applies
                                   its tile to (its metadata and target positions
                                   computed once); 0: chosen from the grid size */

@@ -1,9 +1,9 @@
 """The supernodal solve sweeps in both launch forms against the oracle.
 
-sn_sweep_fused = 1 (default): each sweep is one launch; blocks draw tickets in
-level order and wait, with a bounded wait, until every supernode they solve
-has been released by the blocks that update it.  sn_sweep_fused = 0: one
-launch per sweep level.  Both must give Symbolic_Matrix::solve's result on the
+sn_sweep_fused = 0 (default): one launch per sweep level.  sn_sweep_fused = 1:
+each sweep is one launch; blocks draw tickets in level order and wait, with a
+bounded wait, until every supernode they solve has been released by the
+blocks that update it.  Both must give Symbolic_Matrix::solve's result on the
 same factors (src/symbolic.cc:200-251) within the FP32 solve tolerance, for
 one and for several right-hand sides, and for several value sets at once.
 """
@@ -46,11 +46,13 @@ def test_fused_sweeps_over_value_sets():
     import scipy.sparse as sp
 
     import pyglu
-    from pyglu import synth
+    from pyglu import autotune, synth
 
     A = synth.grid_mesh(side=60, seed=5, n_long=20)
     vals = synth.perturb_values(*A, count=3, seed=2)
     bl = pyglu.BatchedGLU(A[1], A[2], A[3], vals)
+    autotune._set(bl.handle, {"sn_sweep_fused": 1})
+    bl.refactor(vals)
     b = synth.rhs_uniform(A[3], 2, seed=4)
     X = bl.solve(np.broadcast_to(b, (3, 2, A[3])).copy(), tol=1e-12, maxiter=30)
     for z in range(3):
