@@ -1,8 +1,8 @@
 // Trailing update of the dense tail on the 5th-generation tensor cores.
 //
 // The blocked dense LU of the trailing block (glu_factor_dense.cu) spends
-// almost all of its flops in A22 -= L21 U12 with K = 64 or 128 (one panel or a
-// pair), and the deferred coupling of the sparse part adds products of the
+// almost all of its flops in A22 -= L21 U12 with K = 64 .. 256 (one panel or a
+// group of up to four), and the deferred coupling of the sparse part adds products of the
 // same form.  Here that product runs as tcgen05.mma kind::f16 on BF16
 // operands with FP32 accuracy kept by splitting every operand into three BF16
 // parts,
@@ -25,16 +25,15 @@
 
 // Data flow per update:
 //   1. k_dense_pack, after each panel: the panel's L21 rows and U12 columns
-//      split into their three BF16 parts, written K-major as rows of 384
-//      BF16 values (slots 0..127 part 0, 128..255 part 1, 256..383 part 2;
-//      the first panel of a pair fills slots 0..63 of each part, the second
-//      64..127) -- the operand layout the MMA reads.
+//      split into their three BF16 parts, written K-major as rows of 768
+//      BF16 values (slots 0..255 part 0, 256..511 part 1, 512..767 part 2;
+//      panel j of a group fills slots 64 j .. 64 j + 63 of each part) -- the
+//      operand layout the MMA reads.
 //   2. k_dense_update_tc, persistent (one CTA per SM), per 128 x 128 tile of
 //      the trailing block:
 //        warp 0   TMA producer: cp.async.bulk.tensor loads of 128 x 64 BF16
 //                 operand boxes (128-byte swizzle), three parts of A and of B
-//                 per 64-wide K chunk, into a 2-stage ring (a panel pair's
-//                 whole K);
+//                 per 64-wide K chunk (one panel), into a 2-stage ring;
 //        warp 1   MMA issuer: 8 tcgen05.mma (M = N = 128, K = 16) per 16
 //                 of K into one of two accumulator pairs (big, small), the
 //                 pair of the tile before being read meanwhile;
@@ -67,7 +66,8 @@ constexpr int kTile = 128;                               // M = N of an update t
 constexpr int kChunk = 64;                               // K per stage: one 128-byte row of BF16
 constexpr int kStages = 2;
 constexpr int kParts = 3;                                // BF16 parts of an operand
-constexpr int kPackRow = kParts * 128;                   // BF16 values per pack row
+constexpr int kSlots = 256;                              // K slots per part: up to four panels
+constexpr int kPackRow = kParts * kSlots;                // BF16 values per pack row
 constexpr uint32_t kOpBytes = kTile * kChunk * 2;        // one operand part of one stage (16 KB)
 constexpr uint32_t kStageBytes = 2 * kParts * kOpBytes;  // A0, A1, A2, B0, B1, B2
 constexpr int kEpiWarps = 8;                             // two per TMEM lane quarter, 64 columns each
@@ -228,7 +228,7 @@ __device__ __forceinline__ Tile decode_tile(uint32_t t, uint32_t tiles_r, uint32
 // ---------------------------------------------------------------- pack --
 // Rows [r_start, m) of the panel's L21 (columns k0 .. k0 + kb - 1) and
 // columns [r_start, m) of its U12 (rows k0 .. k0 + kb - 1), split into three
-// BF16 parts: pack[z][i][128 * p + slot0 + k] = part p, for k < 64 (zero for
+// BF16 parts: pack[z][i][256 * p + slot0 + k] = part p, for k < 64 (zero for
 // k >= kb).  Blocks [0, nA) take 128 rows of L21 each, the rest 128 columns of
 // U12; blockIdx.z selects the value set.
 __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ val_base, uint64_t stride,
@@ -266,15 +266,15 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
         uint2 p0, p1, p2;
         split_bf16x4(v, p0, p1, p2);
         *reinterpret_cast<uint2 *>(dst + i) = p0;
-        *reinterpret_cast<uint2 *>(dst + 128 + i) = p1;
-        *reinterpret_cast<uint2 *>(dst + 256 + i) = p2;
+        *reinterpret_cast<uint2 *>(dst + kSlots + i) = p1;
+        *reinterpret_cast<uint2 *>(dst + 2 * kSlots + i) = p2;
     }
 }
 
 // ------------------------------------------------------- coupling pack --
 // Operands of one group of deferred sparse columns (up to 128, slots slot0 ..
-// slot0 + ncols - 1): packA[z][i][128 p + s] = part p of L(t + i, k_s),
-// packB[z][j][128 p + s] = part p of U(k_s, t + j), zero where the pattern has
+// slot0 + ncols - 1): packA[z][i][256 p + s] = part p of L(t + i, k_s),
+// packB[z][j][256 p + s] = part p of U(k_s, t + j), zero where the pattern has
 // no entry and for slots past the group.  Block b < nblk takes tail rows
 // [128 b, 128 b + 128): thread s walks column k_s's CSC entries
 // [lstart[g][b], lstart[g][b + 1]) (g = slot0 + s), the ones in those rows.
@@ -322,8 +322,8 @@ __global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restric
         split_bf16x4(v, p0, p1, p2);
         uint16_t *dst = pack + (size_t(blockIdx.z) * m + b0 + r) * kPackRow + 4 * q;
         *reinterpret_cast<uint2 *>(dst) = p0;
-        *reinterpret_cast<uint2 *>(dst + 128) = p1;
-        *reinterpret_cast<uint2 *>(dst + 256) = p2;
+        *reinterpret_cast<uint2 *>(dst + kSlots) = p1;
+        *reinterpret_cast<uint2 *>(dst + 2 * kSlots) = p2;
     }
 }
 
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     mbar_arrive_expect_tx(&full[s], kStageBytes);
 #pragma unroll
                     for (int p = 0; p < kParts; ++p) {
-                        const int x = int(p * 128 + kc * kChunk);
+                        const int x = int(p * kSlots + kc * kChunk);
                         tma_load_3d(st + p * kOpBytes, &mapA, &full[s], x, ya, zz);
                         tma_load_3d(st + (kParts + p) * kOpBytes, &mapB, &full[s], x, yb, zz);
                     }
@@ -679,7 +679,7 @@ cudaError_t launch_tc(const CUtensorMap &mapA, const CUtensorMap &mapB, float *v
     const uint32_t tiles_r = (rows + kTile - 1) / kTile, tiles_c = (cols + kTile - 1) / kTile;
     const uint64_t total = uint64_t(tiles_r) * tiles_c * count;
     if (total == 0 && !reg.writeback) return cudaSuccess;
-    if (r0 > m || total > 0xFFFFFFFFull || nchunks == 0 || nchunks * kChunk > 128) return cudaErrorInvalidValue;
+    if (r0 > m || total > 0xFFFFFFFFull || nchunks == 0 || nchunks * kChunk > kSlots) return cudaErrorInvalidValue;
     uint32_t grid = uint32_t(std::min<uint64_t>(std::max<uint64_t>(total, 1), num_sms));
     if (reg.writeback) grid = std::max<uint32_t>(grid, std::min<uint32_t>(count, num_sms));
     e = cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);

@@ -1047,7 +1047,7 @@ Status create_handle(int device, SymbolicData &&s, uint32_t batch, glu_handle_t 
     h->batch = batch;
     h->pat = std::move(s);
     h->tune = glu_tuning{200000u, 16u, 0u, 64u, 4096u, 128u, 4u, kSnMaxWidth, 1u, kLookaheadMin, kDenseTcMin, 0u, 0u,
-                         0u, 1u};
+                         0u, 1u, kDenseGroupMax};
     const SymbolicData &p = h->pat;
     GLU_CUDA(upload(h->d_cptr, p.sym_c_ptr), "upload pattern");
     GLU_CUDA(upload(h->d_ridx, p.sym_r_idx), "upload pattern");
@@ -1644,13 +1644,14 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
                    launch_dense_gather(h->P, val, stride, count, h->t, h->m, h->d_tail_start.as<uint32_t>(), dbase, st),
                    "factor (dense gather)");
     // Small trailing blocks: panel, update, one panel at a time.  Large ones
-    // (tune.dense_lookahead columns or more) take the panels in pairs: panel
-    // k0, the second panel's row and column strips of its update (K = 64),
-    // panel k0 + 64, then one update of the rest with both panels (K = 128:
-    // every entry still receives its products in column order, C read and
-    // written once per pair).  The panels and the strips run on a
-    // high-priority internal stream, the rest of the pair's update on st,
-    // concurrently with the next pair's first panel, which it does not touch;
+    // (tune.dense_lookahead columns or more) take the panels in groups of
+    // tune.dense_group: panel k0, then for each further panel j of the group
+    // its row and column strips updated by panels 0 .. j - 1 (K = 64 j) and
+    // panel j itself, then one update of the rest with the whole group (K =
+    // 64 x group: every entry still receives its products in column order,
+    // C read and written once per group).  The panels and the strips run on a
+    // high-priority internal stream, the rest of the group's update on st,
+    // concurrently with the next group's first panel, which it does not touch;
     // the next strips wait for it (the same entries, updated in column order).
     const bool lookahead = h->aux && h->tune.dense_lookahead && h->m >= h->tune.dense_lookahead && h->m > kDenseNB;
     const uint32_t *doff = h->d_doff.as<uint32_t>();
@@ -1726,8 +1727,8 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         ++nlaunch;
         return e;
     };
-    // BF16 three-part operands of panel k0 (slot0 0: first of a pair or alone; 64:
-    // second of a pair), on the panel stream
+    // BF16 three-part operands of panel k0 (slot0 = 64 j for panel j of a
+    // look-ahead group), on the panel stream
     auto pack = [&](uint32_t k0, uint32_t kb, uint32_t slot0, bool needed) -> cudaError_t {
         if (!needed) return cudaSuccess;
         cudaError_t e = pf.begin(ps);
@@ -1746,6 +1747,10 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
         nlaunch += dense_panel_launches(count, h->m, k0, kb, h->num_sms);
         return e;
     };
+    // panels per look-ahead group: the group's rest takes K = 64 x group
+    const uint32_t group = lookahead ? std::min<uint32_t>(std::max<uint32_t>(h->tune.dense_group, 2u),
+                                                          kDenseGroupMax)
+                                     : 1u;
     for (uint32_t k0 = 0; k0 < h->m;) {
         const uint32_t kb0 = std::min<uint32_t>(nb, h->m - k0);
         const uint32_t rest0 = h->m - (k0 + kb0);
@@ -1754,44 +1759,48 @@ Status factor_enqueue(glu_handle_s *h, uint32_t first, uint32_t count, int pertu
             GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
             rest_pending = false;
         }
-        const bool single = rest0 <= nb || !lookahead;
-        // packs are written when any update of this step reads them: the
-        // single update, or one of the pair's strips and rest
-        bool packed = false;
-        if (single) {
-            packed = tc_region(rest0, rest0);
-        } else {
-            const uint32_t q1 = k0 + nb, qb1 = std::min<uint32_t>(nb, h->m - q1), r1 = h->m - (q1 + qb1);
-            packed = tc_region(nb, rest0) || tc_region(rest0 - nb, nb) ||
-                     (r1 <= nb ? tc_region(r1, r1)
-                               : (tc_region(nb, r1) || tc_region(r1 - nb, nb) || tc_region(r1 - nb, r1 - nb)));
-        }
-        // after the previous pair's update, which reads the packs
+        // panels of this group: all but the last are full width
+        const uint32_t g = std::min<uint32_t>(group, (h->m - k0 + nb - 1) / nb);
+        // packs are written when any update of this group may read them: every
+        // region of the group lies in the trailing block from k0 on
+        const bool packed = tc_region(h->m - k0, h->m - k0);
+        // after the previous group's update, which reads the packs
         GLU_CUDA(pack(k0, kb0, 0, packed), "factor (dense pack)");
-        if (single) {  // small trailing blocks, last panels: plain steps
+        if (g == 1) {  // small trailing blocks, last panels: plain steps
             GLU_CUDA(update(k0, kb0, DenseRegion{0, rest0, 0, rest0, 1, k0}, ps), "factor (dense update)");
             k0 += kb0;
             continue;
         }
-        // the second panel's strips, then the second panel
-        const uint32_t k1 = k0 + nb, kb1 = std::min<uint32_t>(nb, h->m - k1);
-        GLU_CUDA(update(k0, kb0, DenseRegion{0, nb, 0, rest0, 1, k0}, ps), "factor (dense update)");
-        GLU_CUDA(update(k0, kb0, DenseRegion{nb, rest0, 0, nb, 0, k0}, ps), "factor (dense update)");
-        GLU_CUDA(panel(k1, kb1), "factor (dense panel)");
-        GLU_CUDA(pack(k1, kb1, kDenseNB, packed), "factor (dense pack)");
-        const uint32_t rest1 = h->m - (k1 + kb1), kk = kb0 + kb1;
+        // panel j of the group: its row and column strips take the updates of
+        // panels 0 .. j - 1 (K = 64 j; the first launch after panel j - 1
+        // writes its diagonal block back), then the panel itself
+        uint32_t kk = kb0;  // K of the group so far
+        for (uint32_t j = 1; j < g; ++j) {
+            const uint32_t kj = k0 + kk, kbj = std::min<uint32_t>(nb, h->m - kj), tj = h->m - kj;
+            const uint32_t hj = std::min<uint32_t>(nb, tj);
+            GLU_CUDA(update(k0, kk, DenseRegion{0, hj, 0, tj, 1, kj - nb}, ps), "factor (dense update)");
+            if (tj > hj) GLU_CUDA(update(k0, kk, DenseRegion{hj, tj, 0, hj, 0, kj - nb}, ps), "factor (dense update)");
+            GLU_CUDA(panel(kj, kbj), "factor (dense panel)");
+            GLU_CUDA(pack(kj, kbj, kDenseNB * j, packed), "factor (dense pack)");
+            kk += kbj;
+        }
+        // the rest with the whole group (K = kk): the next group's first panel
+        // strips on the panel stream, the remainder on st concurrently with
+        // that panel
+        const uint32_t kl = k0 + kk - std::min<uint32_t>(nb, kk - (g - 1) * nb);  // last panel of the group
+        const uint32_t rest1 = h->m - (k0 + kk);
         if (rest1 <= nb) {
-            GLU_CUDA(update(k0, kk, DenseRegion{0, rest1, 0, rest1, 1, k1}, ps), "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{0, rest1, 0, rest1, 1, kl}, ps), "factor (dense update)");
         } else {
             GLU_CUDA(cudaEventRecord(h->ev_panel, ps), "event");
-            GLU_CUDA(update(k0, kk, DenseRegion{0, nb, 0, rest1, 1, k1}, ps), "factor (dense update)");
-            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, 0, nb, 0, k1}, ps), "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{0, nb, 0, rest1, 1, kl}, ps), "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, 0, nb, 0, kl}, ps), "factor (dense update)");
             GLU_CUDA(cudaStreamWaitEvent(st, h->ev_panel, 0), "stream wait");
-            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, nb, rest1, 0, k1}, st), "factor (dense update)");
+            GLU_CUDA(update(k0, kk, DenseRegion{nb, rest1, nb, rest1, 0, kl}, st), "factor (dense update)");
             GLU_CUDA(cudaEventRecord(h->ev_rest, st), "event");
             rest_pending = true;
         }
-        k0 = k1 + kb1;
+        k0 += kk;
     }
     if (lookahead) {
         if (rest_pending) GLU_CUDA(cudaStreamWaitEvent(ps, h->ev_rest, 0), "stream wait");
@@ -2207,6 +2216,8 @@ glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t) {
         return set_error(GLU_ERR_ARG, "group_lanes must be 0 or a power of two in [4, 32]");
     if (t->chain_cluster > 16) return set_error(GLU_ERR_ARG, "chain_cluster must be <= 16");
     if (t->solve_cluster > 16) return set_error(GLU_ERR_ARG, "solve_cluster must be <= 16");
+    if (t->dense_group < 2 || t->dense_group > kDenseGroupMax)
+        return set_error(GLU_ERR_ARG, "dense_group must be in [2, %u]", kDenseGroupMax);
     DeviceGuard g(h->device);
     h->tune = *t;
     if (h->tune.chain_cluster) h->chain_cluster = h->tune.chain_cluster;

@@ -102,8 +102,8 @@ cudaError_t launch_dense_panel(float *val, uint64_t stride, uint32_t count, cons
 // Launches one panel step makes: 2 when its blocks over all value sets fill
 // several waves (the diagonal blocks factored once in a launch of their own).
 uint32_t dense_panel_launches(uint32_t count, uint32_t m, uint32_t k0, uint32_t kb, uint32_t num_sms);
-// Part of the trailing update after the panels [k0, k0 + kb) (kb <= 2 x
-// kDenseNB): rows [r_lo, r_hi) and columns [c_lo, c_hi) of the trailing block
+// Part of the trailing update after the panels [k0, k0 + kb) (kb <=
+// kDenseGroupMax x kDenseNB): rows [r_lo, r_hi) and columns [c_lo, c_hi) of the trailing block
 // (relative to k0 + kb); writeback != 0 also stores the factored diagonal
 // block of the panel at wb_k0 from diag_scratch.
 struct DenseRegion {
@@ -113,12 +113,13 @@ cudaError_t launch_dense_update(float *val, uint64_t stride, uint32_t count, con
                                 uint32_t m, uint32_t k0, uint32_t kb, const float *diag_scratch,
                                 DenseRegion reg, cudaStream_t st);
 // The same update on the tensor cores (glu_dense_tc.cu): the panels' L21 rows
-// and U12 columns are first packed as three BF16 parts (pack[z][i][384], one
-// row per trailing row or column, part p at 128 p; the first panel of a pair
-// in slots 0..63, the second in 64..127), then tiles of the region are
-// computed by tcgen05 from TMA loads of the packs.  dense_tc_tensor_map
+// and U12 columns are first packed as three BF16 parts (pack[z][i][768], one
+// row per trailing row or column, part p at 256 p; panel j of a look-ahead
+// group in slots 64 j .. 64 j + 63), then tiles of the region are computed by
+// tcgen05 from TMA loads of the packs (K up to 256).  dense_tc_tensor_map
 // describes a pack buffer of `batch` value sets for the loads.
-constexpr uint32_t kDensePackRow = 384;  // BF16 values (three parts of 128 slots)
+constexpr uint32_t kDensePackRow = 768;  // BF16 values (three parts of 256 slots)
+constexpr uint32_t kDenseGroupMax = 4;   // panels of a look-ahead group (K = 64 x 4)
 constexpr uint32_t kTcTile = 128;  // update tile of the tensor-core kernel (M = N)
 cudaError_t dense_tc_tensor_map(uint16_t *pack, uint32_t m, uint32_t batch, CUtensorMap *map);
 cudaError_t launch_dense_pack(const float *val, uint64_t stride, uint32_t count, const uint32_t *doff, uint32_t m,

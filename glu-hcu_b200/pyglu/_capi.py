@@ -85,7 +85,7 @@ class Tuning(C.Structure):
                 ("solve_cluster", C.c_uint32), ("sn_width", C.c_uint32),
                 ("sn_small", C.c_uint32), ("dense_lookahead", C.c_uint32), ("dense_tc_min", C.c_uint32),
                 ("dense_rate", C.c_uint32), ("sn_sweep_fused", C.c_uint32),
-                ("batch_tile", C.c_uint32), ("defer_tail", C.c_uint32)]
+                ("batch_tile", C.c_uint32), ("defer_tail", C.c_uint32), ("dense_group", C.c_uint32)]
 
 
 _vp = C.c_void_p

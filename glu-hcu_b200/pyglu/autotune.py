@@ -14,7 +14,8 @@ factorization path in use reads --
   small supernodes into warps, the split between sparse part and dense
   trailing block (the cost model's dense rate and the largest buffered
   block), the width from which the dense block takes its panels in
-  look-ahead pairs, the width from which it updates on the tensor cores,
+  look-ahead groups and the panels per group, the width from which it
+  updates on the tensor cores,
   how many of the sparse part's updates of the dense block are deferred to
   tensor-core products after the sparse part;
 * column path (sn_width = 0): lanes per update, the cluster size of the
@@ -46,6 +47,7 @@ SUPERNODAL_SPACE = {
     "dense_lookahead": [0, 1024, 3072],
     "dense_tc_min": [0, 512, 1024, 2048],
     "defer_tail": [0, 1, 4],
+    "dense_group": [2, 3, 4],
 }
 COLUMN_SPACE = {
     "group_lanes": [0, 8, 32],

@@ -319,6 +319,11 @@ typedef struct {
                                   defer_tail scattered entry updates (1: the
                                   built-in estimate; larger values defer more);
                                   0: every supernode scatters its own update    */
+    uint32_t dense_group;      /* panels per look-ahead group of the dense trailing
+                                  block (2..4): panel j of a group first takes the
+                                  updates of panels 0..j-1 on its row and column,
+                                  and the rest of the block then one update of
+                                  K = 64 x group (fewer reads and writes of it) */
 } glu_tuning;
 glu_status glu_get_tuning(glu_handle_t h, glu_tuning *t);
 glu_status glu_set_tuning(glu_handle_t h, const glu_tuning *t);

@@ -175,3 +175,21 @@ def test_deferred_coupling_over_value_sets():
         _capi.check(_capi.engine().glu_store_lu_values(bl.handle, z, 1, _capi.ptr(v), _capi.GLU_HOST, None))
         ok, err, over, ratio = factor_parity(v, ref, ref64, p["sym_c_ptr"])
         assert ok, (z, err, over, ratio)
+
+
+@pytest.mark.parametrize("group", [2, 3, 4])
+@pytest.mark.parametrize("tc", [128, 0], ids=["tensor_cores", "fma"])
+def test_lookahead_groups_match_oracle(group, tc):
+    """Look-ahead groups of 2..4 panels: panel j's strips take K = 64 j, the
+    rest K = 64 x group (up to 256 pack slots on the tensor-core path; the FMA
+    kernel in 64-wide chunks)."""
+    from pyglu import synth
+
+    A = synth.nodal(3000, seed=12, band=32, n_long=2, unsym_frac=0.1)
+    lu, kt = _factor(A, dense_tc_min=tc, dense_lookahead=256, dense_group=group, defer_tail=0)
+    assert lu.stats["dense_tail"] > 4 * 64
+    if tc:
+        assert kt["k_dense_update_tc"][1] > 0
+    ok, err, over, ratio = _check(lu)
+    print(f"group {group} {'tc' if tc else 'fma'}: max column relative difference {err:.3e} ({over}, {ratio:.2f})")
+    assert ok, (err, over, ratio)
