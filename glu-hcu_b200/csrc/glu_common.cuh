@@ -77,6 +77,29 @@ __device__ __forceinline__ void st_release_gpu(int32_t *p, int32_t v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// x rounded to BF16 (1 + 7 explicit significand bits), ties away from zero,
+// as the bits of an FP32 value whose 16 low bits are zero: half a BF16 unit
+// in the last place added to the magnitude bits, the 16 bits below it cleared
+// (a carry into the exponent is the correct rounding up).  Done on the bits so
+// that every part of the split is exact; finite inputs.
+__device__ __forceinline__ uint32_t bf16_rna_bits(float x) { return (__float_as_uint(x) + 0x8000u) & 0xFFFF0000u; }
+
+// The three BF16 parts of four FP32 values, each part's four as one 8-byte
+// word (value u in bits 16 u .. 16 u + 15).
+__device__ __forceinline__ void split_bf16x4(const float (&v)[4], uint2 &p0, uint2 &p1, uint2 &p2) {
+    uint32_t b[3][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        b[0][u] = bf16_rna_bits(v[u]);
+        const float r1 = v[u] - __uint_as_float(b[0][u]);  // exact
+        b[1][u] = bf16_rna_bits(r1);
+        b[2][u] = __float_as_uint(r1 - __uint_as_float(b[1][u]));  // exact, at most 7 significant bits
+    }
+    p0 = make_uint2((b[0][0] >> 16) | (b[0][1] & 0xFFFF0000u), (b[0][2] >> 16) | (b[0][3] & 0xFFFF0000u));
+    p1 = make_uint2((b[1][0] >> 16) | (b[1][1] & 0xFFFF0000u), (b[1][2] >> 16) | (b[1][3] & 0xFFFF0000u));
+    p2 = make_uint2((b[2][0] >> 16) | (b[2][1] & 0xFFFF0000u), (b[2][2] >> 16) | (b[2][3] & 0xFFFF0000u));
+}
+
 // Bounded wait until *cnt reaches target (at most `limit` polls; a wait that
 // sees another wait's timeout in the status word gives up early).  Returns
 // false on timeout, with DEV_TIMEOUT set.

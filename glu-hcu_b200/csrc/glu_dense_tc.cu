@@ -186,29 +186,6 @@ __device__ __forceinline__ void tc_ld32x2(uint32_t ta, uint32_t tb, float (&va)[
     }
 }
 
-// x rounded to BF16 (1 + 7 explicit significand bits), ties away from zero,
-// as the bits of an FP32 value whose 16 low bits are zero: half a BF16 unit
-// in the last place added to the magnitude bits, the 16 bits below it cleared
-// (a carry into the exponent is the correct rounding up).  Done on the bits so
-// that every part of the split is exact; finite inputs.
-__device__ __forceinline__ uint32_t bf16_rna_bits(float x) { return (__float_as_uint(x) + 0x8000u) & 0xFFFF0000u; }
-
-// The three BF16 parts of four FP32 values, each part's four as one 8-byte
-// word (value u in bits 16 u .. 16 u + 15).
-__device__ __forceinline__ void split_bf16x4(const float (&v)[4], uint2 &p0, uint2 &p1, uint2 &p2) {
-    uint32_t b[3][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        b[0][u] = bf16_rna_bits(v[u]);
-        const float r1 = v[u] - __uint_as_float(b[0][u]);  // exact
-        b[1][u] = bf16_rna_bits(r1);
-        b[2][u] = __float_as_uint(r1 - __uint_as_float(b[1][u]));  // exact, at most 7 significant bits
-    }
-    p0 = make_uint2((b[0][0] >> 16) | (b[0][1] & 0xFFFF0000u), (b[0][2] >> 16) | (b[0][3] & 0xFFFF0000u));
-    p1 = make_uint2((b[1][0] >> 16) | (b[1][1] & 0xFFFF0000u), (b[1][2] >> 16) | (b[1][3] & 0xFFFF0000u));
-    p2 = make_uint2((b[2][0] >> 16) | (b[2][1] & 0xFFFF0000u), (b[2][2] >> 16) | (b[2][3] & 0xFFFF0000u));
-}
-
 struct Tile {
     uint32_t z, rbase, cbase;
 };
@@ -276,17 +253,19 @@ __global__ void __launch_bounds__(256) k_dense_pack(const float *__restrict__ va
 // slot0 + ncols - 1): packA[z][i][256 p + s] = part p of L(t + i, k_s),
 // packB[z][j][256 p + s] = part p of U(k_s, t + j), zero where the pattern has
 // no entry and for slots past the group.  Block b < nblk takes tail rows
-// [128 b, 128 b + 128): thread s walks column k_s's CSC entries
+// [128 b, 128 b + 128): four threads of slot s walk column k_s's CSC entries
 // [lstart[g][b], lstart[g][b + 1]) (g = slot0 + s), the ones in those rows.
-// Block nblk + b takes tail columns [128 b, 128 b + 128): thread s walks row
-// k_s's CSR entries [ustart[g][b], ustart[g][b + 1]), the ones in those
-// columns (their CSC positions from cpos).  The start tables (nblk + 1 entries
+// Block nblk + b takes tail columns [128 b, 128 b + 128): four threads of slot
+// s walk row k_s's CSR entries [ustart[g][b], ustart[g][b + 1]), the ones in
+// those columns (their CSC positions from cpos).  The start tables (nblk + 1 entries
 // per slot) are computed with the plan.  A 128 x 128 tile in shared memory,
 // then coalesced writes of the three BF16 parts.
 constexpr uint32_t kCoupleLd = kTile + 1;
 constexpr size_t kCoupleSmem = sizeof(float) * kTile * kCoupleLd;
+constexpr uint32_t kCoupleWalkers = 4;  // threads walking one slot's entries
+constexpr uint32_t kCoupleThreads = kTile * kCoupleWalkers;
 
-__global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restrict__ ridx,
+__global__ void __launch_bounds__(kCoupleThreads) k_couple_pack(const uint32_t *__restrict__ ridx,
                                                        const uint32_t *__restrict__ cidx,
                                                        const uint32_t *__restrict__ cpos,
                                                        const float *__restrict__ val_base, uint64_t stride,
@@ -299,22 +278,25 @@ __global__ void __launch_bounds__(kTile) k_couple_pack(const uint32_t *__restric
     const uint32_t tid = threadIdx.x;
     const bool aside = blockIdx.x < nblk;
     const uint32_t b = aside ? blockIdx.x : blockIdx.x - nblk, b0 = b * kTile;
-    for (uint32_t e = tid; e < kTile * kCoupleLd; e += kTile) sT[e] = 0.0f;
+    for (uint32_t e = tid; e < kTile * kCoupleLd; e += kCoupleThreads) sT[e] = 0.0f;
     __syncthreads();
-    if (tid < ncols) {
-        const uint32_t *st = (aside ? lstart : ustart) + size_t(slot0 + tid) * (nblk + 1) + b;
-        const uint32_t p0 = __ldg(st), p1 = __ldg(st + 1);
+    // kCoupleWalkers threads per slot, each every kCoupleWalkers-th entry
+    const uint32_t sl = tid % kTile, wk = tid / kTile;
+    if (sl < ncols) {
+        const uint32_t *st = (aside ? lstart : ustart) + size_t(slot0 + sl) * (nblk + 1) + b;
+        const uint32_t p0 = __ldg(st) + wk, p1 = __ldg(st + 1);
         if (aside) {
-            for (uint32_t p = p0; p < p1; ++p) sT[(__ldg(ridx + p) - t - b0) * kCoupleLd + tid] = ld_cg(val + p);
+            for (uint32_t p = p0; p < p1; p += kCoupleWalkers)
+                sT[(__ldg(ridx + p) - t - b0) * kCoupleLd + sl] = ld_cg(val + p);
         } else {
-            for (uint32_t e = p0; e < p1; ++e)
-                sT[(__ldg(cidx + e) - t - b0) * kCoupleLd + tid] = ld_cg(val + __ldg(cpos + e));
+            for (uint32_t e = p0; e < p1; e += kCoupleWalkers)
+                sT[(__ldg(cidx + e) - t - b0) * kCoupleLd + sl] = ld_cg(val + __ldg(cpos + e));
         }
     }
     __syncthreads();
     uint16_t *pack = aside ? packA : packB;
     const uint32_t rows = min(uint32_t(kTile), m - b0);
-    for (uint32_t e = tid; e < rows * (kTile / 4); e += kTile) {
+    for (uint32_t e = tid; e < rows * (kTile / 4); e += kCoupleThreads) {
         const uint32_t r = e / (kTile / 4), q = e - r * (kTile / 4);
         const float *src = sT + r * kCoupleLd + 4 * q;
         const float v[4] = {src[0], src[1], src[2], src[3]};
@@ -710,7 +692,7 @@ cudaError_t launch_couple_pack(const DevPattern &P, const float *val, uint64_t s
     });
     if (e != cudaSuccess) return e;
     const uint32_t nblk = (m + kTile - 1) / kTile;
-    k_couple_pack<<<dim3(2 * nblk, 1, count), kTile, kCoupleSmem, st>>>(P.ridx, P.cidx, P.cpos, val, stride, t, m,
+    k_couple_pack<<<dim3(2 * nblk, 1, count), kCoupleThreads, kCoupleSmem, st>>>(P.ridx, P.cidx, P.cpos, val, stride, t, m,
                                                                       ncols, slot0, lstart, ustart, nblk, packA,
                                                                       packB);
     return cudaGetLastError();
