@@ -244,8 +244,8 @@ def run_uneven(args, world, rank, local, pg):
     h2d = sum(v[0].nbytes for v in vals) + sum(b.nbytes for b in bs)
     d2h = sum(x.nbytes for x in xs)
     value = whole_job_value(world, solves, ms)
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": nsteps,
-            "warmup": nwarmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"64 nodal systems, n log-uniform in [2,000, {args.uneven_max_n:,}], "
                                    "1-64 RHS each, refine to 1e-10",

@@ -59,6 +59,11 @@ struct TraceRange {
 // Device allocations still to fail (GLU_INJECT_ALLOC_FAILURES).
 static std::atomic<int> g_fail_allocs{0};
 
+// Bytes of supernode-update position tables held by all handles, per device
+// (their sum is kept under a quarter of the device's memory).
+constexpr int kMaxDevices = 64;
+static std::atomic<uint64_t> g_pos_bytes[kMaxDevices];
+
 static bool injected_alloc_failure() {
     int v = g_fail_allocs.load(std::memory_order_relaxed);
     while (v > 0)
@@ -204,6 +209,7 @@ struct glu_handle_s {
     bool use_sn = false;
     uint32_t nsn = 0;
     DevBuf d_sn_meta, d_sn_dmap, d_sn_dsmall, d_sn_pmap, d_sn_umap, d_sn_psmall, d_sn_usmall, d_sn_tgt_off, d_sn_tgt, d_sn_pos, d_sn_pos_off;
+    uint64_t pos_bytes = 0;  // bytes of d_sn_pos counted in g_pos_bytes
     std::vector<SnLevel> sn_levels;
     SnPlanDev SN{};
     // deferred coupling of the sparse part into the dense tail: per supernode
@@ -260,6 +266,7 @@ struct glu_handle_s {
     glu_stats stats{};
 
     ~glu_handle_s() {
+        if (pos_bytes && device >= 0 && device < kMaxDevices) g_pos_bytes[device] -= pos_bytes;
         if (h_status) cudaFreeHost(h_status);
         if (h_norms) cudaFreeHost(h_norms);
         if (ev0) cudaEventDestroy(ev0);
@@ -677,15 +684,23 @@ Status build_sn_plan(glu_handle_s *h) {
     GLU_CUDA(launch_sn_targets(h->P, h->SN, ns, h->d_sn_tgt.as<uint4>(), 0), "supernode targets");
     GLU_CUDA(cudaDeviceSynchronize(), "supernode targets");
     // Position table of the update scatter, when it fits in a quarter of the
-    // free memory (the values of every value set are allocated by now).
-    // Without it an update entry in a complete in-place dense tail computes
-    // its position, any other searches its target column's rows.
+    // free memory (the values of every value set are allocated by now) and
+    // the tables of all handles on the device stay within a quarter of its
+    // memory (many handles on one GPU must not each claim a quarter of what
+    // is left).  Without it an update entry in a complete in-place dense tail
+    // computes its position, any other searches its target column's rows.
     h->d_sn_pos.release();
+    if (h->pos_bytes && h->device < kMaxDevices) g_pos_bytes[h->device] -= h->pos_bytes;
+    h->pos_bytes = 0;
     const uint64_t entries = pos_off[ns];
+    const uint64_t table_bytes = sizeof(uint32_t) * entries;
     size_t free_b = 0, total_b = 0;
-    if (entries > 0 && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
-        double(entries) * sizeof(uint32_t) <= 0.25 * double(free_b) &&
-        h->d_sn_pos.alloc(sizeof(uint32_t) * entries) == cudaSuccess) {
+    if (entries > 0 && h->device < kMaxDevices && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+        double(table_bytes) <= 0.25 * double(free_b) &&
+        double(g_pos_bytes[h->device].load() + table_bytes) <= 0.25 * double(total_b) &&
+        h->d_sn_pos.alloc(table_bytes) == cudaSuccess) {
+        g_pos_bytes[h->device] += table_bytes;
+        h->pos_bytes = table_bytes;
         GLU_CUDA(launch_sn_positions(h->P, h->SN, ns, h->d_sn_pos.as<uint32_t>(), 0), "supernode positions");
         GLU_CUDA(cudaDeviceSynchronize(), "supernode positions");
         h->SN.pos = h->d_sn_pos.as<uint32_t>();
