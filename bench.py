@@ -660,12 +660,14 @@ def run_ours(args, W, world, rank, local, pg, nsteps, nwarmup, full=True):
         dom_flops = float((2.0 * 64 * 64 * mp).sum()) * B
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     # DRAM traffic per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
-    # over all k_sn_update launches of one factorization of the 300x300 mesh was
-    # 1.171x their algorithmic bytes; the full-size launch is scaled by that
+    # over all k_sn_update launches of a factorization of the 300x300 mesh was
+    # 2.79x their algorithmic bytes (reads; the writes reach DRAM from L2 after
+    # the launches and are not attributed to them); the full-size launch is
+    # scaled by that
     traffic = None
     traffic_note = None
     if dom == "k_sn_update" and dom_n:
-        traffic = 1.171 * dom_bytes / dom_n
+        traffic = 2.79 * dom_bytes / dom_n
         traffic_note = "ncu dram bytes (read+write) of k_sn_update on the 300x300 mesh, scaled by algorithmic bytes"
     sn_alg = {"sn_update_algorithmic_bytes": float(st.sn_update_bytes) * B,
               "sn_update_flops": float(st.sn_update_flops) * B}
