@@ -29,6 +29,24 @@ enum : uint32_t {
     DEV_BAD_INDEX = 8u,
 };
 
+// Launch `kern` on st chained to the previous kernel of the stream (see
+// pdl_release / pdl_wait).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_chained(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                           Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 // Runs a setup step (a kernel attribute: dynamic shared memory above 48 KB, a
 // non-portable cluster size) once per device.  Function attributes belong to
 // the device that was current when they were set, and launchers run on the
@@ -99,6 +117,15 @@ __device__ __forceinline__ void split_bf16x4(const float (&v)[4], uint2 &p0, uin
     p1 = make_uint2((b[1][0] >> 16) | (b[1][1] & 0xFFFF0000u), (b[1][2] >> 16) | (b[1][3] & 0xFFFF0000u));
     p2 = make_uint2((b[2][0] >> 16) | (b[2][1] & 0xFFFF0000u), (b[2][2] >> 16) | (b[2][3] & 0xFFFF0000u));
 }
+
+// Programmatic dependent launch.  A kernel launched with launch_chained may
+// start while the previous kernel of its stream is still running:
+// pdl_release lets the next chained kernel begin launching, pdl_wait blocks
+// until the previous kernel has completed and its writes are visible (a no-op
+// when the kernel was not chained).  Plan data may be read before pdl_wait,
+// anything a previous kernel writes only after it.
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Bounded wait until *cnt reaches target (at most `limit` polls; a wait that
 // sees another wait's timeout in the status word gives up early).  Returns

@@ -284,6 +284,8 @@ __global__ void __launch_bounds__(kTriThreads, 1) k_sn_diag(DevPattern P, SnPlan
                                                             const float *pert_z, uint32_t b0) {
     __shared__ __align__(16) float urow[2][kTriMax];
     __shared__ uint32_t sBase[kSnMaxWidth];
+    pdl_release();
+    pdl_wait();  // the previous level's updates
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
     const uint2 bi = S.dmap[b0 + blockIdx.x];
@@ -322,6 +324,8 @@ __global__ void __launch_bounds__(kSnPanelThreads, 4) k_sn_panel(DevPattern P, S
     float *sF = reinterpret_cast<float *>(snp_sm4);  // L11 column-major (U12 blocks) or U11 row-major (L21 blocks)
     float *sW = sF + kSnMaxWidth * kTriML;           // rows of L21 when w > kTriChunk
     __shared__ uint32_t sOff[kSnMaxWidth];
+    pdl_release();
+    pdl_wait();  // this level's diagonal blocks
     float *val = val_base + blockIdx.z * stride;
     const float pert = pert_z ? pert_z[blockIdx.z] : 0.0f;
     const uint2 bi = S.pmap[b0 + blockIdx.x];
@@ -429,8 +433,10 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
     // value sets [z0, z1) of this block: the tile's metadata and target
     // positions are the same for all of them and computed once
     const uint32_t z0 = blockIdx.z * zpb, z1 = min(z0 + zpb, count);
+    pdl_release();
     const uint2 bi = S.umap[b0 + blockIdx.x];
     if (bi.y & kSnSmallFlag) {  // small supernodes, one per warp
+        pdl_wait();  // this level's panels
         const uint32_t wi = threadIdx.x >> 5;
         if (wi < (bi.y & ~kSnSmallFlag))
             for (uint32_t z = z0; z < z1; ++z)
@@ -517,6 +523,9 @@ __global__ void __launch_bounds__(256, 5) k_sn_update(DevPattern P, SnPlanDev S,
             for (int bb = 0; bb < 4; ++bb)
                 if (r0 + tr * 4 + a >= cu.x && c0 + tc * 4 + bb >= cu.y) pos[a][bb] = 0xffffffffu;
     }
+    // the metadata and positions above are plan data, read while this
+    // level's panels finish; the values only after them
+    pdl_wait();
     for (uint32_t z = z0; z < z1; ++z) {
     float *val = val_base + z * stride;
     if (z > z0) __syncthreads();  // the previous value set's operands are read
@@ -620,8 +629,7 @@ __global__ void __launch_bounds__(256) k_sn_positions(DevPattern P, SnPlanDev S,
 cudaError_t launch_sn_diag(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
                            const float *pert_z, uint32_t b0, uint32_t blocks, cudaStream_t st) {
     if (blocks == 0) return cudaSuccess;
-    k_sn_diag<<<dim3(blocks, 1, count), kTriThreads, 0, st>>>(P, S, val, stride, pert_z, b0);
-    return cudaGetLastError();
+    return launch_chained(k_sn_diag, dim3(blocks, 1, count), dim3(kTriThreads), 0, st, P, S, val, stride, pert_z, b0);
 }
 
 cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
@@ -633,8 +641,8 @@ cudaError_t launch_sn_panel(const DevPattern &P, const SnPlanDev &S, float *val,
     });
     if (e != cudaSuccess) return e;
     const size_t smem = maxw > uint32_t(kTriChunk) ? kSnPanelSmemWide : kSnPanelSmem;
-    k_sn_panel<<<dim3(blocks, 1, count), kSnPanelThreads, smem, st>>>(P, S, val, stride, pert_z, b0);
-    return cudaGetLastError();
+    return launch_chained(k_sn_panel, dim3(blocks, 1, count), dim3(kSnPanelThreads), smem, st, P, S, val, stride, pert_z,
+                          b0);
 }
 
 cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val, uint64_t stride, uint32_t count,
@@ -648,8 +656,8 @@ cudaError_t launch_sn_update(const DevPattern &P, const SnPlanDev &S, float *val
     else
         while (zpb < 8 && zpb * 2 <= count && uint64_t(blocks) * ((count + zpb * 2 - 1) / (zpb * 2)) >= 4ull * 148 * 5)
             zpb *= 2;
-    k_sn_update<<<dim3(blocks, 1, (count + zpb - 1) / zpb), 256, 0, st>>>(P, S, val, stride, b0, atomic, count, zpb);
-    return cudaGetLastError();
+    return launch_chained(k_sn_update, dim3(blocks, 1, (count + zpb - 1) / zpb), dim3(256), 0, st, P, S, val, stride, b0,
+                          atomic, count, zpb);
 }
 
 cudaError_t launch_sn_targets(const DevPattern &P, const SnPlanDev &S, uint32_t nsn, uint4 *tgt, cudaStream_t st) {

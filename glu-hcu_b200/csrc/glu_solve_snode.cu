@@ -158,6 +158,8 @@ __global__ void __launch_bounds__(256, 2) k_sn_sweep_l(DevPattern P, SnSweepPlan
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
                                                     uint64_t vstride, uint64_t ystride, uint32_t *done,
                                                     uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
+    pdl_release();
+    pdl_wait();  // the previous level's x (per-level launches are chained)
     const uint2 bz = sweep_block(W, b0, done, ticket, status, spin_limit);
     const uint32_t blk = bz.x;
     val += bz.y * vstride;  // value set bz.y, its right-hand sides
@@ -242,6 +244,8 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
                                                     float *y, float *xo, uint32_t nrhs, uint32_t b0,
                                                     uint64_t vstride, uint64_t ystride, uint32_t *done,
                                                     uint32_t *ticket, uint32_t *status, uint32_t spin_limit) {
+    pdl_release();
+    pdl_wait();  // the previous level's x (per-level launches are chained)
     const uint2 bz = sweep_block(W, b0, done, ticket, status, spin_limit);
     const uint32_t blk = bz.x;
     val += bz.y * vstride;  // value set bz.y, its right-hand sides
@@ -388,16 +392,20 @@ cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, 
             k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, 0, B.vstride, ystride, done, ticket, status,
                                                spin_limit);
     } else {
+        // one launch per level, each chained to the one before (its blocks
+        // start while the previous level drains, and wait for its x)
         for (uint32_t l = 0; l < W.nlev; ++l) {
             const SnSweepLevel &lv = W.levels[l];
             if (lv.blocks == 0) continue;
             const dim3 grid(lv.blocks, 1, B.count);
+            cudaError_t e;
             if (upper)
-                k_sn_sweep_u<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride, nullptr,
-                                                   nullptr, status, spin_limit);
+                e = launch_chained(k_sn_sweep_u, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
+                                   ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
             else
-                k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, lv.b0, B.vstride, ystride, nullptr,
-                                                   nullptr, status, spin_limit);
+                e = launch_chained(k_sn_sweep_l, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
+                                   ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
+            if (e != cudaSuccess) return e;
         }
     }
     if (t > 0) {  // the vectors of all value sets are contiguous: nrhs * count of them
