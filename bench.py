@@ -261,8 +261,8 @@ def run_uneven(args, world, rank, local, pg):
 
 
 def run_adjoint(args, local):
-    """The differentiation configuration: config-4 generator (band 24, 5%
-    unsymmetric rows) at n = args.adjoint_n, loss = w.x with w standard normal,
+    """The differentiation workload: the nodal generator with band 24 and 5%
+    unsymmetric rows at n = args.adjoint_n, loss = w.x with w standard normal,
     FP32 factor + FP64-refined solve forward, the hand-written adjoint
     (transposed refined solves, -lambda_i x_j on A's pattern) backward.
     Checked against FP64 central differences (relative step 1e-6) on 64
@@ -281,7 +281,7 @@ def run_adjoint(args, local):
     dev = torch.device("cuda", local)
     out = {"metric": "adjoint gradient max relative error vs FP64 central differences", "unit": "relative",
            "higher_is_better": False, "data": "synthetic", "dtype": "f32 factor, f64 refinement",
-           "n_gpus": 1, "config": {"workload": f"config-4 nodal generator n={args.adjoint_n:,}, band 24, "
+           "n_gpus": 1, "config": {"workload": f"nodal generator n={args.adjoint_n:,}, band 24, "
                                                "5% unsymmetric rows, loss w.x"}}
     t0 = time.perf_counter()
     A = synth.config4(n=args.adjoint_n, seed=0)

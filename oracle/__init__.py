@@ -1,7 +1,7 @@
 """Oracle for the GLU numeric path -- TEST INFRASTRUCTURE ONLY.
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
-import this package.  It is the checker, never the thing measured or shipped.
+import this package.  It checks results and is never the thing measured or shipped.
 
 Two parts:
 

@@ -1,4 +1,4 @@
-"""The identities the config-4 finite-difference check evaluates its central
+"""The identities the n = 100,000 finite-difference check evaluates its central
 quotients with, on small dense FP64 systems where subtracting the two
 function values loses nothing:
 

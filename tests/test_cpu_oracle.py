@@ -149,7 +149,7 @@ def test_symbolic_against_oracle_on_meshes():
 
 @pytest.mark.ref
 def test_symbolic_bit_exact_with_reference_config0():
-    """The full-size config-0 matrix (n=4,960): pattern and CSR identical."""
+    """The full-size n=4,960 nodal matrix: pattern and CSR identical."""
     import pyglu
     from pyglu import synth
 
