@@ -450,7 +450,7 @@ def main():
         pg.destroy_process_group()
 
 
-def batch_record(args, world, rank, local, pg, steps=2, warmup=1):
+def batch_record(args, world, rank, local, pg, steps=2, warmup=3):
     """The batched same-pattern workload (256 value sets of one n = 20,000
     pattern, 4 right-hand sides each) at a couple of steps, with the plain
     per-matrix FP32 form beside it, as a sub-record of the default line."""
