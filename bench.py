@@ -80,47 +80,129 @@ def workload(name, side=700, batch=256):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and clock-event reasons of this rank's GPU, sampled
+    during the timed region.
+
+    NVML is polled every 10 ms from a thread, so a timed region of a few
+    hundred milliseconds still gets a dozen readings, plus one reading at
+    start and one at stop.  The device is found by the PCI bus id of the CUDA
+    device, so the reading is of the GPU the kernels run on whatever device
+    numbering CUDA_VISIBLE_DEVICES sets.  Without NVML the same fields come
+    from ``nvidia-smi -lms 200``.  Only reads: nothing here sets a clock."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    PERIOD_S = 0.010
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []          # (sm_mhz, max_mhz, watts, {reason names})
         self.proc = None
+        self.nvml = None
+        self.handle = None
+        self.source = None
+        self.halt = threading.Event()
+        self.thread = None
+
+    def _bus_id(self):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:
+            return None
+
+    def _nvml_sample(self):
+        nv, h = self.nvml, self.handle
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                          float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)),
+                          nv.nvmlDeviceGetPowerUsage(h) / 1e3,
+                          {n for n, b in zip(self.NAMES, bits) if mask & b}))
+
+    def _nvml_loop(self):
+        while not self.halt.wait(self.PERIOD_S):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def start(self):
+        bus = self._bus_id()
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nvml = nv
+            try:
+                self.handle = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.handle = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self._nvml_sample()
+            self.source = "nvml"
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
+            self.rows = []
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={bus or self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.source = "nvidia-smi"
+            self.thread = threading.Thread(target=self._smi_read, daemon=True)
             self.thread.start()
         except OSError:
             self.proc = None
 
-    def _read(self):
+    def _smi_read(self):
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
         for line in self.proc.stdout:
-            self.rows.append([c.strip() for c in line.split(",")])
+            r = [c.strip() for c in line.split(",")]
+            if len(r) < 9:
+                continue
+            self.rows.append((num(r[1]), num(r[2]), num(r[3]),
+                              {n for i, n in enumerate(self.NAMES) if r[5 + i] == "Active"}))
 
     def stop(self):
-        if not self.proc:
+        if self.nvml is not None:
+            self.halt.set()
+            self.thread.join(timeout=5)
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+        elif self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+        else:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
         if not self.rows:
             return None
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        sm = [r[0] for r in self.rows if r[0] is not None]
+        mx = [r[1] for r in self.rows if r[1] is not None]
+        w = [r[2] for r in self.rows if r[2] is not None]
+        reasons = sorted(set().union(*(r[3] for r in self.rows)))
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "sm_min_mhz": min(sm) if sm else None,
+                "power_w_median": float(np.median(w)) if w else None,
+                "reasons": reasons, "samples": len(self.rows), "source": self.source}
 
 
 def dist_setup(args):
