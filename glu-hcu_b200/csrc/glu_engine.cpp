@@ -768,9 +768,10 @@ Status build_sn_plan(glu_handle_s *h) {
                 if (smap.size() + work > UINT32_MAX) return set_error(GLU_ERR_UNSUPPORTED, "solve schedule too large");
                 for (uint64_t bb = 0; bb < work; ++bb) smap.push_back(make_uint2(i, uint32_t(bb)));
             }
+            const uint32_t big = uint32_t(smap.size()) - b0;
             for (size_t g = small0; g < ssmall.size(); g += 8)
                 smap.push_back(make_uint2(uint32_t(g), kSnSmallFlag | uint32_t(std::min<size_t>(8, ssmall.size() - g))));
-            h->ss_levels[u].push_back(SnSweepLevel{b0, uint32_t(smap.size()) - b0});
+            h->ss_levels[u].push_back(SnSweepLevel{b0, uint32_t(smap.size()) - b0, big});
         }
         // fused form: per block the supernodes it solves (waits for) and the
         // supernodes whose unknowns its scatter updates (releases)
@@ -1175,7 +1176,10 @@ uint64_t solve_kernel_count(const glu_handle_s *h, bool trans) {
         const bool sn = !trans && S.sn[u].nlev;
         if (sn) {
             uint32_t lev = 0;
-            for (uint32_t l = 0; l < S.sn[u].nlev; ++l) lev += S.sn[u].levels[l].blocks ? 1 : 0;
+            for (uint32_t l = 0; l < S.sn[u].nlev; ++l) {
+                const uint2 k2 = sn_sweep_level_launches(S.sn[u].levels[l], u == 1);
+                lev += k2.x + k2.y;
+            }
             k += (S.sn[u].fused && h->use_sn ? 1 : lev) + (S.t > 0 ? 1 : 0);
         } else {
             const int mode = trans ? (u == 0 ? SWEEP_UT : SWEEP_LT) : (u == 0 ? SWEEP_L : SWEEP_U);

@@ -206,10 +206,27 @@ constexpr uint32_t kSweepChunk = 128;
 // Supernodal L or U sweep (used when the factor is supernodal): per block of
 // the sweep (levels one after another) its supernode and part, per supernode
 // (sweep order) its record {first column, width, L: first L21 position,
-// L: L21 rows}; the host-side levels.
+// L: L21 rows}; the host-side levels.  A level's blocks are its supernodes'
+// parts first, then its groups of small supernodes.
 struct SnSweepLevel {
     uint32_t b0, blocks;  // first block, blocks
+    uint32_t big;         // blocks [b0, b0 + big) are supernode parts, the rest small groups
 };
+// Blocks of small-supernode groups from which a per-level sweep gives them a
+// launch of their own: a warp-per-supernode kernel that keeps four (L) or
+// five (U) blocks per SM resident, against the full kernel's two (L) or four
+// (U).  The thresholds are where the waves saved on 148 SMs outweigh one more
+// chained launch; below them the level stays one launch.
+constexpr uint32_t kSnSweepSplitL = 592;
+constexpr uint32_t kSnSweepSplitU = 2048;
+// Launches of one level of a per-level sweep: {full kernel, small-group kernel}.
+inline uint2 sn_sweep_level_launches(const SnSweepLevel &lv, bool upper) {
+    const uint32_t small = lv.blocks - lv.big;
+    if (lv.blocks == 0) return {0u, 0u};
+    if (lv.big == 0) return {0u, 1u};
+    if (small >= (upper ? kSnSweepSplitU : kSnSweepSplitL)) return {1u, 1u};
+    return {1u, 0u};
+}
 struct SnSweepPlan {
     const uint2 *map = nullptr;     // {supernode, part} or {first of small[], kSnSmallFlag | count}
     const uint4 *meta = nullptr;

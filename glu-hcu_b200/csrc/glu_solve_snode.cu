@@ -370,6 +370,38 @@ __global__ void __launch_bounds__(256, 4) k_sn_sweep_u(DevPattern P, SnSweepPlan
     sweep_release(W, blk, done);
 }
 
+// Per-level launches of the small-supernode groups alone: blocks
+// [b0, b0 + gridDim.x) of the map are all groups, one small supernode per
+// warp.  Without the full kernels' 64-wide register rows and shared tiles
+// four (L: 64 registers) or five (U: 48) blocks stay resident per SM instead of
+// two or four, so the wide first levels of the L sweep (a quarter of a million
+// leaf supernodes on the 700 x 700 mesh) take half the waves.  Each warp's
+// chain is latency-bound (plan, pattern and factor loads, then w dependent
+// steps), so resident warps set the rate.
+__global__ void __launch_bounds__(256, 4) k_sn_sweep_l_small(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+                                                          float *y, float *xo, uint32_t nrhs, uint32_t b0,
+                                                          uint64_t vstride, uint64_t ystride) {
+    pdl_release();
+    pdl_wait();  // the previous level's x
+    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint32_t wi = threadIdx.x >> 5;
+    if (!(bi.y & kSnSmallFlag) || wi >= (bi.y & ~kSnSmallFlag)) return;
+    sn_sweep_l_small(P, W, val + blockIdx.z * vstride, y + blockIdx.z * ystride, xo + blockIdx.z * ystride, nrhs,
+                     W.small[bi.x + wi], threadIdx.x & 31);
+}
+
+__global__ void __launch_bounds__(256, 5) k_sn_sweep_u_small(DevPattern P, SnSweepPlan W, const float *__restrict__ val,
+                                                          float *y, float *xo, uint32_t nrhs, uint32_t b0,
+                                                          uint64_t vstride, uint64_t ystride) {
+    pdl_release();
+    pdl_wait();  // the previous level's x
+    const uint2 bi = W.map[b0 + blockIdx.x];
+    const uint32_t wi = threadIdx.x >> 5;
+    if (!(bi.y & kSnSmallFlag) || wi >= (bi.y & ~kSnSmallFlag)) return;
+    sn_sweep_u_small(P, W, val + blockIdx.z * vstride, y + blockIdx.z * ystride, xo + blockIdx.z * ystride, nrhs,
+                     W.small[bi.x + wi], threadIdx.x & 31);
+}
+
 __global__ void k_sn_copy(const float *__restrict__ xo, float *y, uint32_t t, uint32_t n) {
     const size_t off = size_t(blockIdx.y) * n;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < t; j += gridDim.x * blockDim.x) y[off + j] = xo[off + j];
@@ -392,20 +424,35 @@ cudaError_t run_sn_sweep(const DevPattern &P, const SnSweepPlan &W, bool upper, 
             k_sn_sweep_l<<<grid, 256, 0, st>>>(P, W, val, y, xo, nrhs, 0, B.vstride, ystride, done, ticket, status,
                                                spin_limit);
     } else {
-        // one launch per level, each chained to the one before (its blocks
-        // start while the previous level drains, and wait for its x)
+        // one launch per level (two where its small-supernode groups get
+        // their own), each chained to the one before (its blocks start while
+        // the previous launch drains, and wait for its x); the supernodes of
+        // one level do not feed each other, so its two launches may run in
+        // either order
         for (uint32_t l = 0; l < W.nlev; ++l) {
             const SnSweepLevel &lv = W.levels[l];
-            if (lv.blocks == 0) continue;
-            const dim3 grid(lv.blocks, 1, B.count);
-            cudaError_t e;
-            if (upper)
-                e = launch_chained(k_sn_sweep_u, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
-                                   ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
-            else
-                e = launch_chained(k_sn_sweep_l, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
-                                   ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
-            if (e != cudaSuccess) return e;
+            const uint2 k2 = sn_sweep_level_launches(lv, upper);
+            cudaError_t e = cudaSuccess;
+            if (k2.x) {  // the full kernel: the parts, and the groups unless they launch apart
+                const dim3 grid(k2.y ? lv.big : lv.blocks, 1, B.count);
+                if (upper)
+                    e = launch_chained(k_sn_sweep_u, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
+                                       ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
+                else
+                    e = launch_chained(k_sn_sweep_l, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs, lv.b0, B.vstride,
+                                       ystride, (uint32_t *)nullptr, (uint32_t *)nullptr, status, spin_limit);
+                if (e != cudaSuccess) return e;
+            }
+            if (k2.y) {  // the small-supernode groups
+                const dim3 grid(lv.blocks - lv.big, 1, B.count);
+                if (upper)
+                    e = launch_chained(k_sn_sweep_u_small, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs,
+                                       lv.b0 + lv.big, B.vstride, ystride);
+                else
+                    e = launch_chained(k_sn_sweep_l_small, grid, dim3(256), 0, st, P, W, val, y, xo, nrhs,
+                                       lv.b0 + lv.big, B.vstride, ystride);
+                if (e != cudaSuccess) return e;
+            }
         }
     }
     if (t > 0) {  // the vectors of all value sets are contiguous: nrhs * count of them

@@ -58,6 +58,29 @@ def test_mesh700_factors_match_reference_numeric_cu():
     assert err <= TOL, err
 
 
+def test_mesh700_plain_solve_matches_oracle_solve():
+    """The FP32 solve of the 700 x 700 mesh (per-level sweeps; its first L
+    level holds about a quarter of a million leaf supernodes, run in their own
+    warp-per-supernode launches) against Symbolic_Matrix::solve's restatement
+    (src/symbolic.cc:200-251) on the same factors."""
+    import pyglu
+    from pyglu import synth
+
+    from test_gpu_sweeps import _oracle_x, split_levels
+
+    A = synth.config1()
+    lu = pyglu.GLUFactorization(*A)
+    b = synth.rhs_loads(A[3], seed=1)[None, :]
+    x = lu.solve(b.T).T
+    splits = split_levels(lu)
+    print("levels with small-group launches:", splits)
+    assert splits >= 0, splits
+    xo = _oracle_x(lu, b)
+    rel = np.abs(x - xo).max() / np.abs(xo).max()
+    print(f"max difference relative to max |x|: {rel:.3e}")
+    assert rel <= TOL, (rel, splits)
+
+
 def test_batch_pattern_factors_match_oracle():
     """Two value sets of the n = 20,000 batched pattern (two, not 256: the
     oracle's FP32 restatement takes about a minute per set on the host)."""

@@ -42,6 +42,38 @@ def test_sweeps_match_oracle(name, fused):
     assert np.abs(x - xo).max() <= TOL * np.abs(xo).max()
 
 
+def split_levels(lu):
+    """Levels of the last plain solve whose small-supernode groups had a launch
+    of their own: the solve's launches less one per sweep level, the two
+    transforms, the two sweeps' copies of the solved unknowns and, with a dense
+    tail, its two triangular sweeps and the tail coupling."""
+    st = lu.stats
+    base = 2 + st["sn_sweep_levels"] + 2 + (3 if st["dense_tail"] else 0)
+    return st["solve_launches"] - base
+
+
+def test_per_level_sweeps_with_small_group_launches_match_oracle():
+    """The 300 x 300 mesh (n = 90,000; tens of thousands of leaf supernodes):
+    the per-level sweeps run the small-supernode groups of the wide levels in
+    their own warp-per-supernode launches, the rest in the full kernel."""
+    import pyglu
+    from pyglu import autotune, synth
+
+    A = synth.config1(side=300)
+    lu = pyglu.GLUFactorization(*A)
+    autotune._set(lu.handle, {"sn_sweep_fused": 0})
+    lu.refactor(A[0])
+    b = synth.rhs_uniform(A[3], 2, seed=9)
+    x = lu.solve(b.T).T
+    splits = split_levels(lu)
+    print("levels with small-group launches:", splits)
+    assert splits >= 0, splits
+    xo = _oracle_x(lu, b)
+    rel = np.abs(x - xo).max() / np.abs(xo).max()
+    print(f"max difference relative to max |x|: {rel:.3e}")
+    assert rel <= TOL, (rel, splits)
+
+
 def test_fused_sweeps_over_value_sets():
     import scipy.sparse as sp
 
