@@ -301,7 +301,10 @@ typedef struct {
                                   model assumes; 0: built in (FMA or tensor-core
                                   rate, whichever the block would use)           */
     uint32_t sn_sweep_fused;   /* 0 (default): one launch per supernodal solve
-                                  sweep level; 1: each sweep is one launch in
+                                  sweep level (a second one for the groups of
+                                  small supernodes of a wide level, or only
+                                  that one where the level has nothing else);
+                                  1: each sweep is one launch in
                                   which a supernode waits (bounded) for the ones
                                   that update it (slower on the patterns
                                   measured: the ticket and the waits cost more
